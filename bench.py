@@ -1,0 +1,457 @@
+"""Benchmark of the halo-finding hot path: peak finding + radial-shell collapse.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tile1152|box512|box128] [--mode batched|plain]
+
+Metric: candidate peaks per second carried through peak finding (all filters, mask
+carried) and the radial-shell collapse, for one tile per GPU (weak scaling: N GPUs run N
+independent tiles, no collective on the data path).  A step is one tile's halo-finding
+stage as run_multitile_split performs it (MultiResolution.jl:1015-1219): per filter the
+cuFFT smoothing (outside this library, as in the reference) and the library's peak scan,
+then the cell-record pack and the shell collapse of every peak in one launch.
+
+Inputs are seeded synthetic fields (BBKS LambdaCDM, Threefry noise, 2LPT), generated on
+the device before timing; they are far larger than the 126 MB L2, so no flush is needed.
+`--impl reference` times the CPU oracle (the C restatement of RadialShell.analyse_peak
+and PeakFind.find_peaks) on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (box cells per side, box size Mpc/h, nbuff, nfilters, Rmin, Rmax)
+    "tile1152": dict(n=1024, L=1500.0, nbuff=64, nf=80, rmin=1.5, rmax=80.0,
+                     desc="1024^3 core + 64-cell buffer = 1152^3 tile, L=1500 Mpc/h, "
+                          "80 top-hat filters R=1.5-80 Mpc/h"),
+    "box512": dict(n=512, L=1000.0, nbuff=54, nf=60, rmin=1.5, rmax=60.0,
+                   desc="512^3 periodic box + 54-cell wrap = 620^3 tile, L=1000 Mpc/h, "
+                        "60 top-hat filters R=1.5-60 Mpc/h"),
+    "box128": dict(n=128, L=250.0, nbuff=36, nf=30, rmin=2.0, rmax=40.0,
+                   desc="128^3 periodic box + 36-cell wrap = 200^3 tile, L=250 Mpc/h, "
+                        "30 top-hat filters R=2-40 Mpc/h"),
+}
+METRIC = "peaks/s thru peakfind+shell collapse"
+UNIT = "peaks/s"
+
+
+def _package():
+    name = "huntian_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    pkg_dir = os.path.join(ROOT, "huntian.jl_b200")
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(pkg_dir, "__init__.py"), submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _peaks_json():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs"), "measured"
+    return 6650.0, "fallback"
+
+
+def _profile_traffic(workload):
+    """Per-launch DRAM bytes of the walk kernel from a committed ncu summary, scaled to
+    the walked cells of this run (the summary stores bytes per walked cell)."""
+    p = os.path.join(ROOT, "profiles", "walk_traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(workload) or d.get("default")
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (start before, stop after)."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [ln.split(",") for ln in open(self.f.name).read().splitlines() if ln.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# --------------------------------------------------------------------- inputs ----
+
+def make_inputs(ht, wl, seed, device):
+    """Synthetic tile: delta, psi1, psi2 on the periodic box, wrapped to the tile, plus
+    delta_k of the box for the per-filter smoothing."""
+    import torch
+    from huntian_b200 import synth
+    n, L, nbuff = wl["n"], wl["L"], wl["nbuff"]
+    cosmo = synth.Cosmology()
+    dk = synth.gaussian_box(n, L, seed, cosmo, device)
+    psi1, psi2 = synth.displacements(dk, n, L, ilpt=2)
+    tile = {"delta": synth.wrap_pad(synth._irfft(dk, n), nbuff)}
+    for nm, t in zip(("etax", "etay", "etaz"), psi1):
+        tile[nm] = synth.wrap_pad(t, nbuff)
+    for nm, t in zip(("eta2x", "eta2y", "eta2z"), psi2):
+        tile[nm] = synth.wrap_pad(t, nbuff)
+    del psi1, psi2
+    torch.cuda.empty_cache()
+    return dk, tile
+
+
+class Workload:
+    def __init__(self, ht, name, seed, device, mode):
+        import torch
+        self.ht, self.name, self.wl, self.mode = ht, name, WORKLOADS[name], mode
+        wl = self.wl
+        self.device = device
+        self.n, self.nbuff = wl["n"], wl["nbuff"]
+        self.nt = self.n + 2 * self.nbuff
+        self.alatt = wl["L"] / self.n
+        self.filters = ht.log_filterbank(wl["nf"], wl["rmin"], wl["rmax"])
+        tab, axes = ht.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+        self.nhunt = ht.nhunt_of(self.filters[0][2], self.alatt, self.nbuff)
+        self.finder = ht.HaloFinder(self.nhunt, tab, *axes, device=device.index or 0)
+        self.ZZon = 1.0                                   # z = 0
+        self.fcrit = float(np.float32(self.finder.fsc_of_z(0.0)))
+        self.dk, self.tile = make_inputs(ht, wl, seed, device)
+        self.mask = torch.zeros((self.nt,) * 3, dtype=torch.int8, device=device)
+        self.max_peaks = 16_000_000 if self.n >= 1024 else 4_000_000
+        self.peaks = ht.HaloFinder.alloc_peaks(self.max_peaks, device, False)
+        self.Rf_f = torch.tensor([f[2] for f in self.filters], dtype=torch.float64, device=device)
+        self.ir2_f = torch.tensor([ht.ir2min_of(f[2], self.alatt) for f in self.filters],
+                                  dtype=torch.int32, device=device)
+        self.results = None
+        self.npeaks = 0
+
+    def smooth(self, Rf):
+        from huntian_b200 import synth
+        return synth.smooth_padded(self.dk, self.n, self.wl["L"], Rf, 1, self.nbuff)
+
+    def step(self, ev=None):
+        """One tile: peak scan over all filters, then pack + shell collapse."""
+        import torch
+        self.mask.zero_()
+        self.peaks["count"].zero_()
+        self.peaks["found"].zero_()
+        for fi, flt in enumerate(self.filters, start=1):
+            ds = self.smooth(flt[2])
+            if ev is not None:
+                ev["pf"][fi - 1][0].record()
+            self.finder.peakfind_filter(ds, self.mask, self.nbuff, self.fcrit, fi,
+                                        self.max_peaks, self.peaks)
+            if ev is not None:
+                ev["pf"][fi - 1][1].record()
+            del ds
+        npk = int(self.peaks["count"].item())
+        self.npeaks = npk
+        self.mask.zero_()                                # MultiResolution.jl:1083
+        t = self.tile
+        if ev is not None:
+            ev["pack"][0].record()
+        self.finder.bind_fields(t["delta"], t["etax"], t["etay"], t["etaz"], t["eta2x"],
+                                t["eta2y"], t["eta2z"], None)
+        if ev is not None:
+            ev["pack"][1].record()
+        fidx = self.peaks["filter_idx"][:npk].long() - 1
+        Rf = self.Rf_f[fidx]
+        ir2 = self.ir2_f[fidx]
+        zz = torch.full((npk,), self.ZZon, dtype=torch.float32, device=self.device)
+        fc = torch.full((npk,), self.fcrit, dtype=torch.float32, device=self.device)
+        if self.results is None or self.results["RTHL"].numel() < npk:
+            self.results = self.ht.HaloFinder.alloc_results(npk, self.device)
+        if ev is not None:
+            ev["walk"][0].record()
+        self.finder.analyse(self.peaks["i"][:npk], self.peaks["j"][:npk],
+                            self.peaks["k"][:npk], Rf, ir2, zz, fc, self.alatt,
+                            nbuff=self.nbuff, mask=self.mask, mode=self.mode,
+                            out=self.results)
+        if ev is not None:
+            ev["walk"][1].record()
+        return npk
+
+
+def run_ours(args, rank, world, device):
+    import torch
+    ht = _package()
+    seed = args.seed + rank
+    W = Workload(ht, args.workload, seed, device, args.mode)
+    dist = world > 1
+    for _ in range(args.warmup):
+        W.step()
+    torch.cuda.synchronize()
+    stats = W.finder.last_stats()
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(device.index or 0) if rank == 0 else None
+    nf = len(W.filters)
+    mk = lambda: torch.cuda.Event(enable_timing=True)
+    evs = [{"pf": [(mk(), mk()) for _ in range(nf)], "pack": (mk(), mk()),
+            "walk": (mk(), mk())} for _ in range(args.steps)]
+    start, end = mk(), mk()
+    start.record()
+    tot_peaks = 0
+    for s in range(args.steps):
+        tot_peaks += W.step(evs[s])
+    end.record()
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ck = clocks.stop() if clocks else None
+    t_ms = start.elapsed_time(end)
+    pf_ms = sum(a.elapsed_time(b) for e in evs for a, b in e["pf"]) / args.steps
+    pack_ms = sum(e["pack"][0].elapsed_time(e["pack"][1]) for e in evs) / args.steps
+    walk_ms = sum(e["walk"][0].elapsed_time(e["walk"][1]) for e in evs) / args.steps
+    if dist:
+        t = torch.tensor([t_ms, float(tot_peaks)], dtype=torch.float64, device=device)
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(t[1:], op=torch.distributed.ReduceOp.SUM)
+        t_ms, tot_peaks = float(tmax[0]), int(t[1])
+    ms_per_step = t_ms / args.steps
+    value = tot_peaks / (t_ms / 1e3)
+
+    # e2e through the public mirror with host buffers (rank 0 measures, all ranks run)
+    e2e = run_e2e(ht, W, args) if args.e2e_steps > 0 else None
+
+    if rank != 0:
+        return None
+    peak_bw, peak_kind = _peaks_json()
+    cells = stats["cells_walked"]
+    alg_bytes = 32.0 * cells + 4.0 * 40 * W.npeaks   # 8 FP32 values per walked cell + outputs
+    achieved = alg_bytes / (walk_ms / 1e3) / 1e9
+    traffic = _profile_traffic(args.workload)
+    if traffic is not None:
+        traffic = float(traffic) * cells
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 sums (Kahan) + f64 collapse",
+        "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
+        "config": {"workload": args.workload, "desc": W.wl["desc"], "mode": args.mode,
+                   "peaks_per_step": W.npeaks, "nhunt": W.nhunt, "nshells": W.finder.nshells,
+                   "fcrit": W.fcrit, "l2": "inputs (43 GB of fields) >> 126 MB L2, no flush",
+                   "parallelism": f"tile-per-GPU x{world}"},
+        "breakdown_ms": {"peakfind_kernels": pf_ms, "pack": pack_ms, "shell_walk": walk_ms,
+                         "smoothing_fft_and_rest": ms_per_step - pf_ms - pack_ms - walk_ms},
+        "hot_path_peaks_per_s": W.npeaks / ((pf_ms + pack_ms + walk_ms) / 1e3),
+        "roofline": {"kernel": "walk_kernel", "bound": "hbm", "achieved": achieved,
+                     "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
+                     "peak_source": peak_kind, "traffic": traffic,
+                     "alg_bytes_per_launch": alg_bytes, "cells_walked": cells},
+        "gpu_launches": int(args.steps * (4 * nf + 1 + 1)),
+        "clocks": ck,
+        "e2e": e2e,
+    }
+    line["cpu_baseline"] = cpu_baseline(ht, W, args) if args.cpu_seconds > 0 else None
+    return line
+
+
+def run_e2e(ht, W, args):
+    """Same step through the public host-buffer API: fields start in pinned host memory,
+    are copied to the device inside the timed region, and all results (peaks, the 14
+    result arrays and the mask) are read back."""
+    import torch
+    host = {k: v.cpu().pin_memory() for k, v in W.tile.items()}
+    dk_host = W.dk.cpu().pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in host.values()) + \
+        dk_host.numel() * dk_host.element_size()
+    d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    tot = 0
+    for _ in range(args.e2e_steps):
+        W.dk = dk_host.to(W.device, non_blocking=True)
+        for k, v in host.items():
+            W.tile[k] = v.to(W.device, non_blocking=True)
+        npk = W.step()
+        tot += npk
+        outs = [W.peaks[c][:npk].cpu() for c in ("i", "j", "k", "delta", "filter_idx")]
+        outs += [W.results[n][:npk * ht.RESULT_WIDTH.get(n, 1)].cpu() for n in ht.RESULT_NAMES]
+        outs.append(W.mask.cpu())
+        d2h = sum(o.numel() * o.element_size() for o in outs)
+    s1.record()
+    torch.cuda.synchronize()
+    ms = s0.elapsed_time(s1)
+    return {"value": tot / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms / args.e2e_steps,
+            "wall_s": time.perf_counter() - t0}
+
+
+def cpu_baseline(ht, W, args, steps=1):
+    """Time the CPU oracle on host cores on a bounded sample of this workload:
+    (a) RadialShell.analyse_peak on a random sample of the step's peaks, all threads;
+    (b) PeakFind.find_peaks on a 128^3 sub-block of every filter's smoothed field.
+    Per-peak CPU time = shell time per peak + (scan time per cell x tile cells x filters)
+    / peaks."""
+    import torch
+    import oracle
+    oracle.build()
+    nthreads = oracle.max_threads()
+    npk = W.npeaks
+    rng = np.random.default_rng(0)
+    budget = args.cpu_seconds
+    # --- shell collapse sample
+    sl = {k: v.cpu().numpy() for k, v in W.tile.items()}
+    F = oracle.Fields(sl["delta"], sl["etax"], sl["etay"], sl["etaz"], sl["eta2x"], sl["eta2y"],
+                      sl["eta2z"])
+    tab, axes = ht.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+    ct = oracle.CollapseTable(tab, *axes)
+    shells = oracle.precompute_shells(W.nhunt)
+    pi = W.peaks["i"][:npk].cpu().numpy(); pj = W.peaks["j"][:npk].cpu().numpy()
+    pk = W.peaks["k"][:npk].cpu().numpy(); fi = W.peaks["filter_idx"][:npk].cpu().numpy() - 1
+    Rf_all = np.array([f[2] for f in W.filters]); ir2_all = W.ir2_f.cpu().numpy()
+    sample, t_shell = 0, 0.0
+    batch = max(4 * nthreads, 64)
+    order = rng.permutation(npk)
+    pos = 0
+    while t_shell < budget * 0.6 and pos < npk:
+        idx = order[pos:pos + batch]
+        pos += len(idx)
+        t0 = time.perf_counter()
+        oracle.analyse_batch(F, pi[idx], pj[idx], pk[idx], ir2_all[fi[idx]], Rf_all[fi[idx]],
+                             W.ZZon, -1.0, W.alatt, ct, shells, nbuff=W.nbuff,
+                             kind="radialshell", nthreads=nthreads)
+        t_shell += time.perf_counter() - t0
+        sample += len(idx)
+        batch = min(batch * 2, 4096)
+    per_peak_shell = t_shell / max(sample, 1)
+    # --- peak scan sample: a 130^3 sub-block (128^3 scanned) of each smoothed field
+    b = 130
+    t_find, nfilt = 0.0, 0
+    mask = np.zeros((b, b, b), np.int8)
+    c0 = W.nbuff
+    for flt in W.filters[:: max(1, len(W.filters) // 8)]:
+        ds = W.smooth(flt[2])[c0:c0 + b, c0:c0 + b, c0:c0 + b].cpu().numpy()
+        t0 = time.perf_counter()
+        oracle.find_peaks(ds, mask, 1, W.fcrit)
+        t_find += time.perf_counter() - t0
+        nfilt += 1
+        if t_find > budget * 0.3:
+            break
+    per_cell = t_find / (nfilt * 128 ** 3)
+    core = W.nt - 2 * W.nbuff
+    find_tile = per_cell * core ** 3 * len(W.filters)
+    cpu_time = per_peak_shell * npk + find_tile
+    return {"value": npk / cpu_time, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"analyse_peak (RadialShell.jl restatement, FP64, {nthreads} threads) on "
+                      f"{sample} random peaks of {npk}; find_peaks on a 128^3 sub-block of "
+                      f"{nfilt} of {len(W.filters)} filters (1 thread), scaled to the tile",
+            "shell_s_per_peak": per_peak_shell, "find_s_per_cell": per_cell}
+
+
+def run_reference(args, rank, world, device):
+    """--impl reference: the CPU oracle on the host cores, on bounded samples."""
+    if rank != 0:
+        return None
+    import torch
+    ht = _package()
+    W = Workload(ht, args.workload, args.seed, device, "batched")
+    W.step()
+    torch.cuda.synchronize()
+    vals = []
+    for s in range(args.warmup + args.steps):
+        cb = cpu_baseline(ht, W, argparse.Namespace(cpu_seconds=args.ref_seconds))
+        if s >= args.warmup:
+            vals.append(cb)
+    v = float(np.mean([c["value"] for c in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * W.npeaks / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
+            "config": {"workload": args.workload, "desc": W.wl["desc"],
+                       "peaks_per_step": W.npeaks},
+            "impl": "reference", "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tile1152", choices=list(WORKLOADS))
+    ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--seed", type=int, default=12345)
+    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    if args.impl == "reference":
+        line = run_reference(args, rank, world, device)
+    else:
+        line = run_ours(args, rank, world, device)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+"""ctypes bindings of libhuntian_b200.so (include/huntian_b200.h).
+
+The library is the product: every compute entry point of this package goes through it.
+If it is missing or fails to load, import of the bindings raises -- there is no CPU or
+PyTorch fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhuntian_b200.so")
+
+HT_OK = 0
+HT_ERR_INVALID = 1
+HT_ERR_CUDA = 2
+HT_ERR_NOMEM = 3
+HT_ERR_STATE = 4
+HT_ERR_CAPACITY = 5
+HT_ERR_FAULT = 6
+
+HT_CONV_GPU = 0
+HT_CONV_CPU = 1
+HT_MODE_PLAIN = 0
+HT_MODE_BATCHED = 1
+
+# every symbol include/huntian_b200.h declares
+SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
+           "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_peakfind_filter", "ht_fields_pack",
+           "ht_shell_analyse", "ht_last_launch_stats")
+
+
+class HTError(RuntimeError):
+    """A huntian_b200 entry point returned a non-zero status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"huntian_b200 error {code}: {msg}")
+        self.code = code
+
+
+_P = C.c_void_p
+
+
+class HtPeaks(C.Structure):
+    _fields_ = [("i", _P), ("j", _P), ("k", _P), ("delta", _P), ("lapd", _P),
+                ("filter_idx", _P), ("count", _P), ("found", _P)]
+
+
+class HtFields(C.Structure):
+    _fields_ = [("delta", _P), ("etax", _P), ("etay", _P), ("etaz", _P), ("eta2x", _P),
+                ("eta2y", _P), ("eta2z", _P), ("lapd", _P), ("n1", C.c_int32),
+                ("n2", C.c_int32), ("n3", C.c_int32)]
+
+
+class HtPeakBatch(C.Structure):
+    _fields_ = [("pi", _P), ("pj", _P), ("pk", _P), ("Rf", _P), ("ir2min", _P), ("ZZon", _P),
+                ("fcrit", _P), ("npeaks", C.c_int64)]
+
+
+RESULT_NAMES = ("RTHL", "Fbarx", "e_v", "p_v", "strain", "eigs", "Srb", "Sbar", "Sbar2",
+                "gradpk", "gradpkf", "gradpkrf", "d2F", "zvir_half")
+RESULT_WIDTH = {"strain": 9, "eigs": 3, "Sbar": 3, "Sbar2": 3, "gradpk": 3, "gradpkf": 3,
+                "gradpkrf": 3}
+
+
+class HtResults(C.Structure):
+    _fields_ = [(n, _P) for n in RESULT_NAMES]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libhuntian_b200.so (built by build.py); raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with "
+                          "`python huntian.jl_b200/build.py` (no fallback path exists)")
+    L = C.CDLL(LIB_PATH)
+    i32, i64, dbl = C.c_int32, C.c_int64, C.c_double
+    L.ht_last_error.restype = C.c_char_p
+    L.ht_last_error.argtypes = []
+    L.ht_ctx_create.restype = C.c_int
+    L.ht_ctx_create.argtypes = [C.c_int, C.c_int, _P, C.c_int, C.c_int, C.c_int, dbl, dbl,
+                                dbl, dbl, dbl, dbl, dbl, C.POINTER(_P)]
+    L.ht_ctx_destroy.restype = C.c_int
+    L.ht_ctx_destroy.argtypes = [_P]
+    L.ht_ctx_shell_info.restype = C.c_int
+    L.ht_ctx_shell_info.argtypes = [_P, C.POINTER(i32), C.POINTER(i64)]
+    L.ht_ctx_shell_r2.restype = C.c_int
+    L.ht_ctx_shell_r2.argtypes = [_P, _P, i32]
+    L.ht_fsc_of_z.restype = C.c_int
+    L.ht_fsc_of_z.argtypes = [_P, dbl, C.POINTER(dbl)]
+    L.ht_peakfind_filter.restype = C.c_int
+    L.ht_peakfind_filter.argtypes = [_P, _P, _P, _P, C.c_int, C.c_int, C.c_float, i32, i64,
+                                     C.POINTER(HtPeaks), _P]
+    L.ht_fields_pack.restype = C.c_int
+    L.ht_fields_pack.argtypes = [_P, C.POINTER(HtFields), _P]
+    L.ht_shell_analyse.restype = C.c_int
+    L.ht_shell_analyse.argtypes = [_P, C.POINTER(HtPeakBatch), dbl, dbl, i32, _P, i32, i32,
+                                   C.POINTER(HtResults), _P]
+    L.ht_last_launch_stats.restype = C.c_int
+    L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != HT_OK:
+        raise HTError(rc, load().ht_last_error().decode(errors="replace"))

@@ -1,0 +1,48 @@
+"""Build recipe for libhuntian_b200.so (sm_100a), in-tree next to this file.
+
+    python huntian.jl_b200/build.py [--verbose]
+
+Compiles every .cu under csrc/ with nvcc for sm_100a only (no fast-math: the collapse
+criterion needs IEEE divisions, square roots and NaN propagation) and links them into
+one shared library with a plain C ABI (include/huntian_b200.h).
+"""
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIB = os.path.join(HERE, "libhuntian_b200.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+         "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-shared",
+         "-cudart", "shared", "-I", os.path.join(ROOT, "include")]
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def deps():
+    return sources() + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + \
+        [os.path.join(ROOT, "include", "huntian_b200.h")]
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    return any(os.path.getmtime(d) > t for d in deps())
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or needs_build():
+        cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + sources() + ["-o", LIB]
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force=True, verbose="--verbose" in sys.argv)
+    print(LIB)

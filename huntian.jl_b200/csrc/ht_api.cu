@@ -1,0 +1,326 @@
+// C ABI of huntian_b200: context management, host-side tables, argument checks and
+// dispatch to the kernels in ht_peakfind.cu and ht_shell.cu.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "ht_internal.cuh"
+
+// ----------------------------------------------------------------- errors ----
+
+static thread_local std::string g_last_error;
+
+int ht_fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int ht_cuda_fail(cudaError_t e, const char* what) {
+    return ht_fail(HT_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+// Host-side fault injection for tests: HT_FAULT_INJECT="alloc" makes every device
+// allocation fail, "launch" makes every kernel dispatch fail, before the device is
+// touched.  Off unless the variable is set.
+bool ht_fault_injected(const char* site) {
+    const char* v = getenv("HT_FAULT_INJECT");
+    if (!v || !*v) return false;
+    std::string s(v);
+    size_t pos = 0;
+    while (pos <= s.size()) {
+        size_t e = s.find(',', pos);
+        if (e == std::string::npos) e = s.size();
+        if (s.compare(pos, e - pos, site) == 0) return true;
+        pos = e + 1;
+    }
+    return false;
+}
+
+int ht_alloc(void** p, size_t bytes, const char* what) {
+    if (ht_fault_injected("alloc")) return ht_fail(HT_ERR_FAULT, std::string("injected allocation fault: ") + what);
+    cudaError_t e = cudaMalloc(p, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        char buf[128];
+        snprintf(buf, sizeof buf, " (%zu bytes)", bytes);
+        return ht_fail(HT_ERR_NOMEM, std::string("cudaMalloc failed for ") + what + buf + ": " +
+                                         cudaGetErrorString(e));
+    }
+    return HT_OK;
+}
+
+int ht_grow(void** p, size_t* have, size_t need, const char* what) {
+    if (*p && *have >= need) return HT_OK;
+    if (*p) { cudaFree(*p); *p = nullptr; *have = 0; }
+    int rc = ht_alloc(p, need, what);
+    if (rc == HT_OK) *have = need;
+    return rc;
+}
+
+extern "C" const char* ht_last_error(void) { return g_last_error.c_str(); }
+
+// ------------------------------------------------------------ host tables ----
+
+// Shell offsets (RadialShell.jl:151-166): all (di, dj, dk) with r^2 <= nhunt^2, in
+// dk-outer / dj / di-inner generation order, stably sorted by r^2 (a counting sort is
+// stable), grouped into shells by r^2 (ShellAnalysisGPU.jl:44-71).
+static void build_shells(ht_ctx* c, int nhunt) {
+    const int r2max = nhunt * nhunt;
+    std::vector<int64_t> hist((size_t)r2max + 2, 0);
+    for (int dk = -nhunt; dk <= nhunt; ++dk)
+        for (int dj = -nhunt; dj <= nhunt; ++dj)
+            for (int di = -nhunt; di <= nhunt; ++di) {
+                int r2 = di * di + dj * dj + dk * dk;
+                if (r2 <= r2max) hist[r2 + 1]++;
+            }
+    std::vector<int64_t> pos(hist.size());
+    int64_t acc = 0;
+    for (size_t r = 0; r + 1 < hist.size(); ++r) { acc += hist[r + 1]; pos[r] = acc - hist[r + 1]; }
+    c->ncells = acc;
+    c->h_off.assign((size_t)acc, make_char4(0, 0, 0, 0));
+    std::vector<int64_t> wr(pos.begin(), pos.end());
+    for (int dk = -nhunt; dk <= nhunt; ++dk)
+        for (int dj = -nhunt; dj <= nhunt; ++dj)
+            for (int di = -nhunt; di <= nhunt; ++di) {
+                int r2 = di * di + dj * dj + dk * dk;
+                if (r2 <= r2max) c->h_off[(size_t)wr[r2]++] = make_char4((signed char)di, (signed char)dj, (signed char)dk, 0);
+            }
+    // shells, 1-based with padding at 0 and nshells + 1
+    c->h_r2.assign(1, 0);
+    c->h_start.assign(1, 0);
+    c->h_count.assign(1, 0);
+    for (int r2 = 0; r2 <= r2max; ++r2) {
+        if (hist[r2 + 1] == 0) continue;
+        c->h_r2.push_back(r2);
+        c->h_start.push_back((int32_t)pos[r2]);
+        c->h_count.push_back((int32_t)hist[r2 + 1]);
+    }
+    c->nshells = (int32_t)c->h_r2.size() - 1;
+    c->h_r2.push_back(INT32_MAX);
+    c->h_start.push_back((int32_t)acc);
+    c->h_count.push_back(0);
+}
+
+// SPH table atab4 (RadialShell.jl:125-142): akk[i] = W(sqrt(u)), u = i * 0.01 (0-based).
+static void build_akk(std::vector<double>& akk) {
+    const double pi = 3.14159265358979323846;
+    const double ca = 3.0 / (2.0 * pi), cb = 1.0 / (4.0 * pi);
+    akk.assign(1101, 0.0);
+    for (int i = 0; i < 1100; ++i) {
+        const double u = i * 0.01, ru = sqrt(u);
+        double v = 0.0;
+        if (ru < 1.0) v = ca * (2.0 / 3.0 - u + 0.5 * u * ru);
+        else if (ru <= 2.0) { const double t = 2.0 - ru; v = cb * (t * t * t); }
+        akk[i] = v;
+    }
+    akk[1100] = 0.0;
+}
+
+// Trilinear lookup on the host copy (CollapseTable.jl:126-138), for fsc_of_z.
+static double host_interp(const ht_ctx* c, double x, double y, double z) {
+    if (!(x >= c->X1 && x <= c->X2 && y >= c->Y1 && y <= c->Y2 && z >= c->Z1 && z <= c->Z2))
+        return c->out_val;
+    double tx = (x - c->X1) / ((c->X2 - c->X1) / (c->nx - 1));
+    double ty = (y - c->Y1) / ((c->Y2 - c->Y1) / (c->ny - 1));
+    double tz = (z - c->Z1) / ((c->Z2 - c->Z1) / (c->nz - 1));
+    int ix = std::min(std::max((int)floor(tx), 0), c->nx - 2);
+    int iy = std::min(std::max((int)floor(ty), 0), c->ny - 2);
+    int iz = std::min(std::max((int)floor(tz), 0), c->nz - 2);
+    double fx = tx - ix, fy = ty - iy, fz = tz - iz;
+    const size_t sy = c->nx, sz = (size_t)c->nx * c->ny;
+    const float* t = c->h_ct.data() + ix + iy * sy + iz * sz;
+    double c00 = t[0] * (1.0 - fx) + t[1] * fx;
+    double c10 = t[sy] * (1.0 - fx) + t[1 + sy] * fx;
+    double c01 = t[sz] * (1.0 - fx) + t[1 + sz] * fx;
+    double c11 = t[sy + sz] * (1.0 - fx) + t[1 + sy + sz] * fx;
+    double c0 = c00 * (1.0 - fy) + c10 * fy;
+    double c1 = c01 * (1.0 - fy) + c11 * fy;
+    return c0 * (1.0 - fz) + c1 * fz;
+}
+
+static void free_ctx(ht_ctx* c) {
+    void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
+                    c->d_rec, c->d_pf_ws, c->d_scratch, c->d_queue, c->d_stats};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete c;
+}
+
+template <typename T>
+static int upload(T** dst, const T* src, size_t n, const char* what) {
+    int rc = ht_alloc((void**)dst, n * sizeof(T), what);
+    if (rc != HT_OK) return rc;
+    HT_CUDA_TRY(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice), what);
+    return HT_OK;
+}
+
+// ------------------------------------------------------------------- ABI ----
+
+extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, int nx, int ny,
+                             int nz, double X1, double X2, double Y1, double Y2, double Z1,
+                             double Z2, double out_val, ht_ctx** out) {
+    if (!out) return ht_fail(HT_ERR_INVALID, "ht_ctx_create: out is NULL");
+    *out = nullptr;
+    if (nhunt < 1 || nhunt > 127)
+        return ht_fail(HT_ERR_INVALID, "ht_ctx_create: nhunt must be in 1..127 (offsets are 8-bit)");
+    if (!ct_table_host || nx < 2 || ny < 2 || nz < 2)
+        return ht_fail(HT_ERR_INVALID, "ht_ctx_create: collapse table must be at least 2x2x2");
+    if (!(X2 > X1) || !(Y2 > Y1) || !(Z2 > Z1))
+        return ht_fail(HT_ERR_INVALID, "ht_ctx_create: collapse-table axes must be increasing");
+    HT_CUDA_TRY(cudaSetDevice(device), "cudaSetDevice");
+    ht_ctx* c = new ht_ctx();
+    c->device = device;
+    c->nhunt = nhunt;
+    cudaError_t e = cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) { free_ctx(c); return ht_cuda_fail(e, "cudaDeviceGetAttribute"); }
+    build_shells(c, nhunt);
+    std::vector<double> rad(c->h_r2.size());
+    for (size_t m = 0; m < rad.size(); ++m)
+        rad[m] = (m == 0 || m + 1 == rad.size()) ? (m == 0 ? 0.0 : INFINITY) : sqrt((double)c->h_r2[m]);
+    c->h_ct.assign(ct_table_host, ct_table_host + (size_t)nx * ny * nz);
+    c->nx = nx; c->ny = ny; c->nz = nz;
+    c->X1 = X1; c->X2 = X2; c->Y1 = Y1; c->Y2 = Y2; c->Z1 = Z1; c->Z2 = Z2;
+    c->out_val = out_val;
+    std::vector<double> akk;
+    build_akk(akk);
+    int rc;
+    if ((rc = upload(&c->d_off, c->h_off.data(), c->h_off.size(), "shell offsets")) ||
+        (rc = upload(&c->d_start, c->h_start.data(), c->h_start.size(), "shell starts")) ||
+        (rc = upload(&c->d_count, c->h_count.data(), c->h_count.size(), "shell counts")) ||
+        (rc = upload(&c->d_r2, c->h_r2.data(), c->h_r2.size(), "shell r2")) ||
+        (rc = upload(&c->d_rad, rad.data(), rad.size(), "shell radii")) ||
+        (rc = upload(&c->d_ct, c->h_ct.data(), c->h_ct.size(), "collapse table")) ||
+        (rc = upload(&c->d_akk, akk.data(), akk.size(), "SPH table")) ||
+        (rc = ht_alloc((void**)&c->d_queue, 256, "work queue")) ||
+        (rc = ht_alloc((void**)&c->d_stats, 256, "launch stats"))) {
+        free_ctx(c);
+        return rc;
+    }
+    HT_CUDA_TRY(cudaMemset(c->d_stats, 0, 256), "stats init");
+    *out = c;
+    return HT_OK;
+}
+
+extern "C" int ht_ctx_destroy(ht_ctx* ctx) {
+    if (!ctx) return HT_OK;
+    cudaSetDevice(ctx->device);
+    free_ctx(ctx);
+    return HT_OK;
+}
+
+extern "C" int ht_ctx_shell_info(const ht_ctx* ctx, int32_t* nshells, int64_t* ncells) {
+    if (!ctx) return ht_fail(HT_ERR_INVALID, "ht_ctx_shell_info: ctx is NULL");
+    if (nshells) *nshells = ctx->nshells;
+    if (ncells) *ncells = ctx->ncells;
+    return HT_OK;
+}
+
+extern "C" int ht_ctx_shell_r2(const ht_ctx* ctx, int32_t* r2_host, int32_t cap) {
+    if (!ctx || !r2_host) return ht_fail(HT_ERR_INVALID, "ht_ctx_shell_r2: NULL argument");
+    if (cap < ctx->nshells) return ht_fail(HT_ERR_CAPACITY, "ht_ctx_shell_r2: cap < nshells");
+    memcpy(r2_host, ctx->h_r2.data() + 1, sizeof(int32_t) * (size_t)ctx->nshells);
+    return HT_OK;
+}
+
+extern "C" int ht_fsc_of_z(const ht_ctx* ctx, double z, double* fcrit_out) {
+    if (!ctx || !fcrit_out) return ht_fail(HT_ERR_INVALID, "ht_fsc_of_z: NULL argument");
+    double target = 1.0 + z, lo = ctx->X1, hi = ctx->X2;
+    for (int it = 0; it < 50; ++it) {
+        double mid = 0.5 * (lo + hi);
+        if (host_interp(ctx, mid, 0.0, 0.0) > target) hi = mid; else lo = mid;
+    }
+    *fcrit_out = pow(10.0, lo);
+    return HT_OK;
+}
+
+extern "C" int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_s,
+                                  int8_t* d_mask, int n, int nbuff, float fcrit,
+                                  int32_t filter_idx, int64_t max_peaks, const ht_peaks* out,
+                                  void* stream) {
+    if (!ctx || !d_delta_s || !d_mask || !out)
+        return ht_fail(HT_ERR_INVALID, "ht_peakfind_filter: NULL argument");
+    if (!out->i || !out->j || !out->k || !out->delta || !out->filter_idx || !out->count)
+        return ht_fail(HT_ERR_INVALID, "ht_peakfind_filter: NULL output array");
+    if (n < 3 || nbuff < 1 || 2 * nbuff >= n)
+        return ht_fail(HT_ERR_INVALID, "ht_peakfind_filter: need n >= 3 and 1 <= nbuff < n/2 "
+                                       "(the 3x3x3 stencil reads one cell beyond the inner cube)");
+    if ((long long)n * n * n > (1LL << 40))
+        return ht_fail(HT_ERR_CAPACITY, "ht_peakfind_filter: n^3 too large");
+    if (max_peaks < 0) return ht_fail(HT_ERR_INVALID, "ht_peakfind_filter: max_peaks < 0");
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_peakfind_filter");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return ht_launch_peakfind(ctx, d_delta_s, d_lapd_s, d_mask, n, nbuff, fcrit, filter_idx,
+                              max_peaks, out, (cudaStream_t)stream);
+}
+
+extern "C" int ht_fields_pack(ht_ctx* ctx, const ht_fields* f, void* stream) {
+    if (!ctx || !f) return ht_fail(HT_ERR_INVALID, "ht_fields_pack: NULL argument");
+    if (!f->delta || !f->etax || !f->etay || !f->etaz)
+        return ht_fail(HT_ERR_INVALID, "ht_fields_pack: delta and eta x/y/z are required");
+    const bool any2 = f->eta2x || f->eta2y || f->eta2z;
+    const bool all2 = f->eta2x && f->eta2y && f->eta2z;
+    if (any2 && !all2) return ht_fail(HT_ERR_INVALID, "ht_fields_pack: give all of eta2x/y/z or none");
+    if (f->n1 < 1 || f->n1 != f->n2 || f->n1 != f->n3)
+        return ht_fail(HT_ERR_INVALID, "ht_fields_pack: the tile must be cubic (the gather reads "
+                                       "delta[k, i, j], ext/CUDAExt.jl:819)");
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_fields_pack");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t cells = (size_t)f->n1 * f->n2 * f->n3;
+    if (!ctx->d_rec || ctx->rec_cells < cells) {
+        if (ctx->d_rec) { cudaFree(ctx->d_rec); ctx->d_rec = nullptr; ctx->rec_cells = 0; }
+        int rc = ht_alloc((void**)&ctx->d_rec, cells * 2 * sizeof(float4), "cell records");
+        if (rc != HT_OK) { ctx->bound = false; return rc; }
+        ctx->rec_cells = cells;
+    }
+    ctx->fields = *f;
+    ctx->bound = true;
+    return ht_launch_pack(ctx, (cudaStream_t)stream);
+}
+
+extern "C" int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* b, double alatt,
+                                double rmax2rs, int32_t nbuff, int8_t* d_mask, int32_t conv,
+                                int32_t mode, const ht_results* out, void* stream) {
+    if (!ctx || !b || !out) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: NULL argument");
+    if (!ctx->bound) return ht_fail(HT_ERR_STATE, "ht_shell_analyse: call ht_fields_pack first");
+    if (b->npeaks < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: npeaks < 0");
+    if (b->npeaks > 0 && (!b->pi || !b->pj || !b->pk || !b->Rf || !b->ir2min || !b->ZZon || !b->fcrit))
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: NULL peak array");
+    if (b->npeaks > 0 && (!out->RTHL || !out->Fbarx || !out->e_v || !out->p_v || !out->strain ||
+                          !out->eigs || !out->Srb || !out->Sbar || !out->Sbar2 || !out->gradpk ||
+                          !out->gradpkf || !out->gradpkrf || !out->d2F || !out->zvir_half))
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: NULL result array");
+    if (!(alatt > 0.0)) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: alatt must be > 0");
+    if (conv != HT_CONV_GPU && conv != HT_CONV_CPU)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: unknown conv");
+    if (conv == HT_CONV_CPU && rmax2rs > 0.0)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: HT_CONV_CPU supports rmax2rs == 0 only");
+    if (mode != HT_MODE_PLAIN && mode != HT_MODE_BATCHED)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: unknown mode");
+    if (nbuff < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: nbuff < 0");
+    if (ctx->nshells < 3) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: hunt radius too small");
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_shell_analyse");
+    ctx->last_kernels = 0;
+    if (b->npeaks == 0) return HT_OK;
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return ht_launch_walk(ctx, b, alatt, rmax2rs, nbuff, d_mask, conv, mode, out,
+                          (cudaStream_t)stream);
+}
+
+extern "C" int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
+                                    int64_t* cells_walked) {
+    if (!ctx) return ht_fail(HT_ERR_INVALID, "ht_last_launch_stats: ctx is NULL");
+    if (kernels) *kernels = ctx->last_kernels;
+    if (shells_walked || cells_walked) {
+        unsigned long long h[2] = {0, 0};
+        HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+        HT_CUDA_TRY(cudaMemcpy(h, ctx->d_stats, sizeof h, cudaMemcpyDeviceToHost), "stats read");
+        if (cells_walked) *cells_walked = (int64_t)h[0];
+        if (shells_walked) *shells_walked = (int64_t)h[1];
+    }
+    return HT_OK;
+}

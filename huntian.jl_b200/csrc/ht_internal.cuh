@@ -1,0 +1,77 @@
+// Internal declarations shared by the huntian_b200 CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "huntian_b200.h"
+
+// ------------------------------------------------------------------ context ----
+
+struct ht_ctx {
+    int device = 0;
+    int num_sms = 0;
+    int nhunt = 0;
+
+    // Shell table (ShellAnalysisGPU.jl:28-71), 1-based by shell index m = 1..nshells:
+    // shell m holds cells [start[m], start[m] + count[m]) of the r^2-sorted cell list.
+    int32_t nshells = 0;
+    int64_t ncells = 0;
+    std::vector<int32_t> h_r2, h_start, h_count;
+    std::vector<char4> h_off;
+    char4* d_off = nullptr;        // (di, dj, dk, 0) per cell, r^2-sorted
+    int32_t* d_start = nullptr;    // [nshells + 2]
+    int32_t* d_count = nullptr;    // [nshells + 2]
+    int32_t* d_r2 = nullptr;       // [nshells + 2]
+    double* d_rad = nullptr;       // sqrt(r2), [nshells + 2]
+
+    // collapse table + SPH table
+    std::vector<float> h_ct;
+    float* d_ct = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+    double X1 = 0, X2 = 0, Y1 = 0, Y2 = 0, Z1 = 0, Z2 = 0, out_val = -1.0;
+    double* d_akk = nullptr;       // 1101 entries
+
+    // bound tile
+    bool bound = false;
+    ht_fields fields{};
+    float4* d_rec = nullptr;       // 2 float4 per cell
+    size_t rec_cells = 0;
+
+    // workspaces
+    void* d_pf_ws = nullptr;       // peak-find bitmap + segment counts
+    size_t pf_ws_bytes = 0;
+    double* d_scratch = nullptr;   // shell-walk per-warp profiles
+    size_t scratch_bytes = 0;
+    int32_t* d_queue = nullptr;    // dynamic work counter
+    unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked
+
+    int64_t last_kernels = 0;
+};
+
+// ----------------------------------------------------------------- errors ----
+
+int ht_fail(int code, const std::string& msg);
+int ht_cuda_fail(cudaError_t e, const char* what);
+bool ht_fault_injected(const char* site);   // HT_FAULT_INJECT=<site>[,<site>...]
+int ht_alloc(void** p, size_t bytes, const char* what);
+int ht_grow(void** p, size_t* have, size_t need, const char* what);
+
+#define HT_CUDA_TRY(call, what)                                   \
+    do {                                                          \
+        cudaError_t _e = (call);                                  \
+        if (_e != cudaSuccess) return ht_cuda_fail(_e, what);     \
+    } while (0)
+
+// ------------------------------------------------------- kernel launchers ----
+
+int ht_launch_pack(ht_ctx* ctx, cudaStream_t st);
+int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_s,
+                       int8_t* d_mask, int n, int nbuff, float fcrit, int32_t filter_idx,
+                       int64_t max_peaks, const ht_peaks* out, cudaStream_t st);
+int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rmax2rs,
+                   int32_t nbuff, int8_t* d_mask, int32_t conv, int32_t mode,
+                   const ht_results* out, cudaStream_t st);

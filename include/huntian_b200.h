@@ -1,0 +1,191 @@
+/*
+ * huntian_b200 -- B200 (sm_100a) kernels for Huntian.jl's halo-finding hot path:
+ * peak finding on the filtered linear density field and the radial-shell
+ * homogeneous-ellipsoid collapse.
+ *
+ * C ABI only: plain pointers, sizes and status codes.  Device pointers are raw CUDA
+ * device addresses (e.g. Julia's pointer(::CuArray), torch's Tensor.data_ptr());
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *
+ * Every entry point returns HT_OK (0) or an error code; ht_last_error() gives the
+ * message of the calling thread's last failure.  Nothing exits or traps.
+ *
+ * Array conventions (the reference's): 3-D fields are Float32, column-major
+ * (i fastest), 1-based (i, j, k) in all index outputs.
+ *
+ * Reference interfaces replaced (guanyilun/Huntian.jl):
+ *   ht_peakfind_filter  -> ext/CUDAExt.jl:2876-2936 `_find_peaks_kernel!` (one filter of
+ *                          the loop at ext/CUDAExt.jl:2985-3012 behind
+ *                          `peak_find_tile_gpu`, stub src/Huntian.jl:387-412)
+ *   ht_fields_pack +
+ *   ht_shell_analyse    -> ext/CUDAExt.jl:2085-2344 `analyse_peaks_gpu_cuda_multirf`
+ *                          (stub src/Huntian.jl:259-281): the gather kernel
+ *                          ext/CUDAExt.jl:752-924 and post-process kernel
+ *                          ext/CUDAExt.jl:1213-1912
+ *   ht_ctx_create       -> per-call uploads of ShellTablesGPU (ext/CUDAExt.jl:16-41), the
+ *                          collapse table and the SPH table (ext/CUDAExt.jl:45-52)
+ *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
+ *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
+ */
+#ifndef HUNTIAN_B200_H
+#define HUNTIAN_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HT_API __attribute__((visibility("default")))
+#else
+#define HT_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define HT_OK 0
+#define HT_ERR_INVALID 1   /* bad argument (null pointer, size, shape) */
+#define HT_ERR_CUDA 2      /* a CUDA runtime call failed */
+#define HT_ERR_NOMEM 3     /* device allocation failed */
+#define HT_ERR_STATE 4     /* call order (e.g. shell analysis before packing fields) */
+#define HT_ERR_CAPACITY 5  /* a size exceeds a documented maximum */
+#define HT_ERR_FAULT 6     /* injected host-side fault (HT_FAULT_INJECT, tests only) */
+
+/* shell-walk conventions (which reference routine the results reproduce) */
+#define HT_CONV_GPU 0      /* analyse_peaks_gpu_cuda_multirf / ShellAnalysisGPU.analyse_peak_gpu
+                              + zvir_half (ext/CUDAExt.jl:1213-1912) */
+#define HT_CONV_CPU 1      /* RadialShell.analyse_peak (src/HaloFinder/RadialShell.jl:281-865):
+                              lagged mrf counter, d2F without the centre cell that stops at the
+                              first out-of-tile cell; requires rmax2rs == 0 */
+
+/* shell-walk execution modes (all return identical results) */
+#define HT_MODE_PLAIN 0    /* per-field gathers, static peak-to-warp schedule */
+#define HT_MODE_BATCHED 1  /* interleaved cell records, persistent kernel, dynamic queue */
+
+typedef struct ht_ctx ht_ctx;
+
+/* Context on one CUDA device: shell tables for hunt radius `nhunt` (cells with
+ * r^2 <= nhunt^2, ShellAnalysisGPU.jl:44-71), the collapse table (host Float32,
+ * column-major nx*ny*nz, axes X1..Z2 as in the HomelTab header, out_val outside the
+ * table: CollapseTable.jl:119-138) and the SPH table atab4 (RadialShell.jl:125-147).
+ * Replaces the per-call uploads at ext/CUDAExt.jl:2128-2141.  nhunt must be 1..127. */
+HT_API int ht_ctx_create(int device, int nhunt, const float* ct_table_host, int nx, int ny, int nz,
+                  double X1, double X2, double Y1, double Y2, double Z1, double Z2,
+                  double out_val, ht_ctx** out);
+HT_API int ht_ctx_destroy(ht_ctx* ctx);
+
+/* Message of this thread's last failed call ("" if none). */
+HT_API const char* ht_last_error(void);
+
+/* Number of shells (distinct r^2, incl. r^2 = 0) and cells of the context's table. */
+HT_API int ht_ctx_shell_info(const ht_ctx* ctx, int32_t* nshells, int64_t* ncells);
+/* Copy the shell r^2 values (nshells entries) to host memory. */
+HT_API int ht_ctx_shell_r2(const ht_ctx* ctx, int32_t* r2_host, int32_t cap);
+
+/* fcrit = 10^x where zvir(x, 0, 0) = 1 + z, by 50 bisection steps on the context's
+ * collapse table (RadialShell.jl:181-195).  Host computation. */
+HT_API int ht_fsc_of_z(const ht_ctx* ctx, double z, double* fcrit_out);
+
+/* ------------------------------------------------------------- peak finding ---- */
+
+/* Output arrays of the peak finder (device memory, capacity max_peaks each).
+ * `count` points to ONE device int64: the running number of stored peaks; it must be
+ * zeroed by the caller before the first filter and is advanced by each call.
+ * `found` (optional, device int64) accumulates all local maxima including those
+ * dropped beyond max_peaks.  lapd may be NULL when no Laplacian field is given. */
+typedef struct {
+    int32_t* i;
+    int32_t* j;
+    int32_t* k;
+    float* delta;       /* delta_s at the peak (FcRf) */
+    float* lapd;        /* lapd_s at the peak (d2Rf), nullable */
+    int32_t* filter_idx;
+    int64_t* count;
+    int64_t* found;     /* nullable */
+} ht_peaks;
+
+/* One filter of the peak scan (PeakFind.jl:15-78 semantics): cells of the inner cube
+ * (nbuff+1 : n-nbuff)^3 with mask != 1, delta_s >= fcrit and no 26-neighbour strictly
+ * above (ties accepted) become peaks, are appended in k/j/i scan order after the
+ * peaks already counted, and get mask = 1.  Peaks beyond max_peaks are neither stored
+ * nor masked.  Unlike the reference GPU kernel the order is deterministic (scan order),
+ * so indices are bit-identical to the CPU peak finder.  d_mask is n^3 Int8 (in/out). */
+HT_API int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_s,
+                       int8_t* d_mask, int n, int nbuff, float fcrit, int32_t filter_idx,
+                       int64_t max_peaks, const ht_peaks* out, void* stream);
+
+/* ------------------------------------------------------------ shell collapse ---- */
+
+/* Tile fields (device, Float32 column-major n1*n2*n3).  eta2* may all be NULL (1LPT:
+ * zeros), lapd may be NULL (ioutshear = 0: d2F = 0).  The transposed read
+ * delta[k, i, j] of the reference gather requires a cubic tile. */
+typedef struct {
+    const float* delta;
+    const float* etax;
+    const float* etay;
+    const float* etaz;
+    const float* eta2x;
+    const float* eta2y;
+    const float* eta2z;
+    const float* lapd;
+    int32_t n1, n2, n3;
+} ht_fields;
+
+/* Bind a tile to the context and build its interleaved cell-record copy
+ * (32 B per cell: delta, delta[k,i,j], eta xyz, eta2 xyz) in context-owned device
+ * memory.  The caller's fields must stay valid until the next ht_fields_pack or
+ * ht_ctx_destroy (PLAIN mode and lapd read them directly). */
+HT_API int ht_fields_pack(ht_ctx* ctx, const ht_fields* fields, void* stream);
+
+/* Peaks to analyse (device arrays of npeaks): 1-based i, j, k; filter radius Rf
+ * (Mpc/h, Float64 as the reference's batch tuples carry it); ir2min = min(floor((1.75 Rf/alatt)^2), floor((40/alatt - 1)^2))
+ * (MultiResolution.jl:575-576); ZZon = 1 + z and fcrit per peak (the broadcast or
+ * lightcone values of ext/CUDAExt.jl:2215-2218). */
+typedef struct {
+    const int32_t* pi;
+    const int32_t* pj;
+    const int32_t* pk;
+    const double* Rf;
+    const int32_t* ir2min;
+    const float* ZZon;
+    const float* fcrit;
+    int64_t npeaks;
+} ht_peak_batch;
+
+/* Per-peak outputs (device, Float32; vectors are (3, npeaks) and strain (3, 3, npeaks)
+ * column-major), the 14 arrays of ext/CUDAExt.jl:2003-2016.  No-collapse peaks get
+ * RTHL = zvir_half = -1 and zeros elsewhere. */
+typedef struct {
+    float* RTHL;
+    float* Fbarx;
+    float* e_v;
+    float* p_v;
+    float* strain;
+    float* eigs;
+    float* Srb;
+    float* Sbar;
+    float* Sbar2;
+    float* gradpk;
+    float* gradpkf;
+    float* gradpkrf;
+    float* d2F;
+    float* zvir_half;
+} ht_results;
+
+/* Radial-shell collapse of every peak of `batch` on the bound tile.  alatt in Mpc/h;
+ * rmax2rs > 0 limits shells to r <= rmax2rs*Rf/alatt (ext/CUDAExt.jl:2192-2200);
+ * d_mask (nullable, n^3 Int8) gets 1 on core cells within RTHL.  conv: HT_CONV_*;
+ * mode: HT_MODE_*.  Results are identical for every mode. */
+HT_API int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* batch, double alatt,
+                     double rmax2rs, int32_t nbuff, int8_t* d_mask, int32_t conv,
+                     int32_t mode, const ht_results* out, void* stream);
+
+/* Launch statistics of the last ht_shell_analyse on this context: kernels launched and
+ * the total number of shells walked (for the roofline's algorithmic bytes). */
+HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
+                         int64_t* cells_walked);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

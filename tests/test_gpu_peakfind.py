@@ -1,0 +1,109 @@
+"""Peak finder on the GPU vs the CPU oracle (PeakFind.jl:15-78): bit-exact indices,
+values, filter indices, order and mask, on the reference's known-answer cases and on
+smoothed random fields with the mask carried across filters."""
+import numpy as np
+import pytest
+
+from gpu_helpers import gpu_find_peaks
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def finder(ht, fortran_table_path):
+    tab, axes = ht.read_homeltab(fortran_table_path)
+    return ht.HaloFinder(4, tab, *axes)
+
+
+def _cell(a, i, j, k, v):
+    a[k - 1, j - 1, i - 1] = v
+
+
+def _both(ht, oracle, finder, fields, nbuff, fcrits, max_peaks=1 << 20, mask=None,
+          lapd=None):
+    n = fields[0].shape[0]
+    mask = np.zeros((n, n, n), np.int8) if mask is None else mask
+    g, gmask = gpu_find_peaks(ht, finder, fields, mask.copy(), nbuff, fcrits, max_peaks,
+                              lapd_s=lapd)
+    om = mask.copy()
+    oi, oj, ok, od, of = [], [], [], [], []
+    left = max_peaks
+    for fi, (ds, fc) in enumerate(zip(fields, fcrits), start=1):
+        if left <= 0:
+            break
+        i, j, k, d = oracle.find_peaks(ds, om, nbuff, fc, left)
+        oi += list(i); oj += list(j); ok += list(k); od += list(d); of += [fi] * len(i)
+        left -= len(i)
+    assert list(g["i"]) == oi and list(g["j"]) == oj and list(g["k"]) == ok
+    assert np.array_equal(g["delta"].view(np.int32), np.asarray(od, np.float32).view(np.int32))
+    assert list(g["filter_idx"]) == of
+    assert np.array_equal(gmask, om)
+    return g
+
+
+def test_reference_kats(ht, oracle, finder):
+    n = 11
+    d = np.zeros((n, n, n), np.float32); _cell(d, 6, 6, 6, 2.0)
+    g = _both(ht, oracle, finder, [d], 1, [1.0])
+    assert list(zip(g["i"], g["j"], g["k"])) == [(6, 6, 6)]
+    _both(ht, oracle, finder, [np.full((n, n, n), 0.5, np.float32)], 1, [1.0])
+    grad = np.fromfunction(lambda k, j, i: i + j + k + 3.0, (n, n, n)).astype(np.float32)
+    assert len(_both(ht, oracle, finder, [grad], 1, [1.0])["i"]) == 0
+    m = np.zeros((n, n, n), np.int8); m[5, 5, 5] = 1
+    assert len(_both(ht, oracle, finder, [d], 1, [1.0], mask=m)["i"]) == 0
+    d2 = np.zeros((n, n, n), np.float32); _cell(d2, 1, 6, 6, 2.0)
+    assert len(_both(ht, oracle, finder, [d2], 1, [1.0])["i"]) == 0
+    n = 15
+    d4 = np.zeros((n, n, n), np.float32)
+    for c in [(4, 4, 4), (4, 4, 12), (12, 12, 4), (12, 12, 12)]:
+        _cell(d4, *c, 2.0)
+    g = _both(ht, oracle, finder, [d4], 1, [1.0], max_peaks=2)
+    assert len(g["i"]) == 2
+
+
+def _smooth_random(n, seed, radii):
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((n, n, n))
+    wk = np.fft.rfftn(w)
+    k = np.sqrt(np.add.outer(np.add.outer(np.fft.fftfreq(n) ** 2, np.fft.fftfreq(n) ** 2),
+                             np.fft.rfftfreq(n) ** 2)) * 2 * np.pi
+    out = []
+    for R in radii:
+        x = k * R
+        with np.errstate(invalid="ignore", divide="ignore"):
+            win = np.where(x == 0, 1.0, 3 * (np.sin(x) - x * np.cos(x)) / x ** 3)
+        f = np.fft.irfftn(wk * win, s=(n, n, n))
+        out.append((f / f.std()).astype(np.float32))
+    return out
+
+
+@pytest.mark.parametrize("n,nbuff", [(48, 4), (45, 3), (70, 1), (37, 5)])
+def test_random_fields_mask_carried(ht, oracle, finder, n, nbuff):
+    fields = _smooth_random(n, n + nbuff, [4.0, 2.5, 1.5, 1.0])
+    g = _both(ht, oracle, finder, fields, nbuff, [1.0, 1.2, 0.5, 0.0])
+    assert len(g["i"]) > 20
+
+
+def test_truncation_across_filters(ht, oracle, finder):
+    fields = _smooth_random(40, 1, [2.0, 1.0])
+    total = len(_both(ht, oracle, finder, fields, 2, [0.0, 0.0])["i"])
+    for mp in (1, 7, total // 2, total - 1):
+        g = _both(ht, oracle, finder, fields, 2, [0.0, 0.0], max_peaks=mp)
+        assert len(g["i"]) == mp
+
+
+def test_ties_and_plateaus(ht, oracle, finder):
+    n = 20
+    d = np.zeros((n, n, n), np.float32)
+    d[5:8, 5:8, 5:8] = 3.0          # a plateau: every cell of it is a peak (ties pass)
+    d[12, 12, 12] = 2.0; d[12, 12, 13] = 2.0
+    g = _both(ht, oracle, finder, [d], 2, [1.0])
+    assert len(g["i"]) == 27 + 2
+
+
+def test_lapd_sampled_at_peaks(ht, oracle, finder):
+    fields = _smooth_random(32, 5, [2.0])
+    lap = _smooth_random(32, 6, [1.0])
+    g = _both(ht, oracle, finder, fields, 2, [0.5], lapd=lap)
+    idx = (g["k"] - 1, g["j"] - 1, g["i"] - 1)
+    assert np.array_equal(g["lapd"], lap[0][idx])
