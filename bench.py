@@ -84,6 +84,11 @@ class Clocks:
     """nvidia-smi sampling during the timed region (start before, stop after)."""
 
     def __init__(self, index):
+        try:
+            import torch
+            index = "GPU-" + str(torch.cuda.get_device_properties(index).uuid)
+        except Exception:
+            pass
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"

@@ -308,20 +308,25 @@ __device__ __forceinline__ Shape shape_of(const double E[6]) {
     return s;
 }
 
-// Transposed butterfly reduction: 32 per-lane values in, lane l returns the warp total
-// of value l.  31 double shuffles; the summation tree is fixed (deterministic).
-__device__ __forceinline__ double warp_transpose_reduce(double (&v)[32], int lane) {
-#pragma unroll
-    for (int w = 16; w >= 1; w >>= 1) {
-        const bool upper = (lane & w) != 0;
-#pragma unroll
-        for (int i = 0; i < w; ++i) {
-            double send = upper ? v[i] : v[i + w];
-            double keep = upper ? v[i + w] : v[i];
-            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, w);
-        }
+// Per-warp shared-memory staging: the 23 per-lane shell sums during the walk, and the
+// results of 32 inward-walk steps (+ one carried step) during the post-processing.
+constexpr int kRedRows = 23, kRedPitch = 33;          // [value][lane], padded pitch
+constexpr int kStepW = 16, kStepRows = 33;            // [lane or carry][field]
+constexpr int kWarpSmemDoubles =
+    kRedRows * kRedPitch > kStepRows * kStepW ? kRedRows * kRedPitch : kStepRows * kStepW;
+
+// Lane v (< 23) returns the warp total of value v, summed over lanes 0..31 in order
+// (deterministic).  `R` is the warp's staging area.
+__device__ __forceinline__ double warp_column_sum(double* R, int lane) {
+    __syncwarp();
+    double s = 0.0;
+    if (lane < kRedRows) {
+        const double* r = R + lane * kRedPitch;
+#pragma unroll 8
+        for (int t = 0; t < 32; ++t) s += r[t];
     }
-    return v[0];
+    __syncwarp();
+    return s;
 }
 
 __device__ __forceinline__ double warp_sum(double x) {
@@ -376,20 +381,6 @@ __device__ __forceinline__ Step eval_step(const WalkArgs& a, const double* P, in
         }
     }
     return st;
-}
-
-__device__ __forceinline__ Step shfl_step(const Step& s, int src) {
-    Step r;
-#pragma unroll
-    for (int i = 0; i < 6; ++i) r.k.E[i] = __shfl_sync(0xffffffffu, s.k.E[i], src);
-#pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        r.k.g[i] = __shfl_sync(0xffffffffu, s.k.g[i], src);
-        r.k.gf[i] = __shfl_sync(0xffffffffu, s.k.gf[i], src);
-    }
-    r.trace = __shfl_sync(0xffffffffu, s.trace, src);
-    r.zvir = __shfl_sync(0xffffffffu, s.zvir, src);
-    return r;
 }
 
 template <bool PACKED>
@@ -453,7 +444,8 @@ __device__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
 }
 
 template <bool PACKED>
-__device__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P, int lane) {
+__device__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P,
+                             double* __restrict__ R, int lane) {
     const double* rad = a.rad;
     const int ci = a.pi[p], cj = a.pj[p], ck = a.pk[p];
     const double Rf = a.Rf[p];
@@ -549,21 +541,18 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
                 for (int K = 0; K < 3; ++K) acc[13 + 3 * L + K].add(v[2 + L] * d[K]);
             }
         }
-        double vals[32];
-        vals[V_F] = acc[0].value();
-        vals[V_N] = (double)nin;
+        R[V_F * kRedPitch + lane] = acc[0].value();
+        R[V_N * kRedPitch + lane] = (double)nin;
 #pragma unroll
         for (int L = 0; L < 3; ++L) {
-            vals[V_S + L] = acc[1 + L].value();
-            vals[V_S2 + L] = acc[4 + L].value();
-            vals[V_G + L] = acc[7 + L].value();
-            vals[V_GF + L] = acc[10 + L].value();
+            R[(V_S + L) * kRedPitch + lane] = acc[1 + L].value();
+            R[(V_S2 + L) * kRedPitch + lane] = acc[4 + L].value();
+            R[(V_G + L) * kRedPitch + lane] = acc[7 + L].value();
+            R[(V_GF + L) * kRedPitch + lane] = acc[10 + L].value();
         }
 #pragma unroll
-        for (int i = 0; i < 9; ++i) vals[V_SR + i] = acc[13 + i].value();
-#pragma unroll
-        for (int i = V_COUNT; i < 32; ++i) vals[i] = 0.0;
-        const double mine = warp_transpose_reduce(vals, lane);
+        for (int i = 0; i < 9; ++i) R[(V_SR + i) * kRedPitch + lane] = acc[13 + i].value();
+        const double mine = warp_column_sum(R, lane);
 
         // finalise shell s (ShellAnalysisGPU.jl:197-228)
         const double Fs = __shfl_sync(0xffffffffu, mine, V_F);
@@ -658,35 +647,43 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
 
     // inward walk (RadialShell.jl:529-686): step t evaluates shell m0 - t; step 0 is
     // m0 itself with zvir forced to -1 (RadialShell.jl:566-567).  Lanes evaluate 32
-    // consecutive steps at once; the first step with zvir >= ZZon collapses.
-    Step last, prev;
-    int tstar = -1;
-    {
-        Step carry;   // last step of the previous group (valid when base > 0)
-        for (int base = 0; base < m0 && tstar < 0; base += 32) {
-            const int t = base + lane;
-            Step mine;
-            if (t < m0) mine = eval_step(a, P, m0 - t, m, t == 0);
-            else { mine.zvir = -1.0; }
-            const bool hit = t < m0 && mine.zvir >= ZZon;
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (bal) {
-                const int l = __ffs(bal) - 1;
-                tstar = base + l;
-                last = shfl_step(mine, l);
-                if (l > 0) prev = shfl_step(mine, l - 1);
-                else prev = carry;
-            } else {
-                carry = shfl_step(mine, 31);
-            }
+    // consecutive steps at once; the first step with zvir >= ZZon collapses.  Step
+    // results are staged in R (row = lane, row 32 = last step of the previous group).
+    int tstar = -1, lrow = 0, prow = 0;
+    for (int base = 0; base < m0; base += 32) {
+        const int t = base + lane;
+        double* row = R + lane * kStepW;
+        bool hit = false;
+        if (t < m0) {
+            const Step st = eval_step(a, P, m0 - t, m, t == 0);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) row[i] = st.k.E[i];
+#pragma unroll
+            for (int i = 0; i < 3; ++i) { row[6 + i] = st.k.g[i]; row[9 + i] = st.k.gf[i]; }
+            row[12] = st.trace;
+            row[13] = st.zvir;
+            hit = st.zvir >= ZZon;
         }
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        __syncwarp();
+        if (bal) {
+            const int l = __ffs(bal) - 1;
+            tstar = base + l;
+            lrow = l;
+            prow = l > 0 ? l - 1 : 32;
+            break;
+        }
+        if (lane < 14) R[32 * kStepW + lane] = R[31 * kStepW + lane];
+        __syncwarp();
     }
     if (tstar < 0 || (tstar == 0 && m0 == 1)) { write_no_collapse(a, p, lane); return; }
-    if (tstar == 0) prev = last;
+    if (tstar == 0) prow = lrow;
+    const double* Lr = R + lrow * kStepW;   // collapse step ("last")
+    const double* Pr = R + prow * kStepW;   // the step before it ("prev")
 
     const int m0f = m0 - tstar + 1;   // collapse at shell mp* = m0f - 1
-    const double zvir1p = last.zvir;
-    const double zvir1 = tstar == 0 ? -1.0 : prev.zvir;
+    const double zvir1p = Lr[13];
+    const double zvir1 = tstar == 0 ? -1.0 : Pr[13];
     const double dZ = zvir1p - zvir1;
     const double rp = rad[m0f - 1], rm = rad[m0f];
     double RTHL;
@@ -707,18 +704,18 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         const double frac = (RTHL3 - rad3p) / drad3;
         Fbarx = Fb_p + frac * (Fb_m - Fb_p);
 #pragma unroll
-        for (int i = 0; i < 6; ++i) smat[i] = last.k.E[i] + frac * (prev.k.E[i] - last.k.E[i]);
+        for (int i = 0; i < 6; ++i) smat[i] = Lr[i] + frac * (Pr[i] - Lr[i]);
 #pragma unroll
         for (int i = 0; i < 3; ++i) {
-            gpk[i] = last.k.g[i] + frac * (prev.k.g[i] - last.k.g[i]);
-            gpkf[i] = last.k.gf[i] + frac * (prev.k.gf[i] - last.k.gf[i]);
+            gpk[i] = Lr[6 + i] + frac * (Pr[6 + i] - Lr[6 + i]);
+            gpkf[i] = Lr[9 + i] + frac * (Pr[9 + i] - Lr[9 + i]);
         }
     } else {
         Fbarx = Fb_p;
 #pragma unroll
-        for (int i = 0; i < 6; ++i) smat[i] = last.k.E[i];
+        for (int i = 0; i < 6; ++i) smat[i] = Lr[i];
 #pragma unroll
-        for (int i = 0; i < 3; ++i) { gpk[i] = prev.k.g[i]; gpkf[i] = prev.k.gf[i]; }
+        for (int i = 0; i < 3; ++i) { gpk[i] = Pr[6 + i]; gpkf[i] = Pr[9 + i]; }
     }
     // normalize_strain + eigen (RadialShell.jl:730-734)
     const double tr = smat[0] + smat[1] + smat[2];
@@ -730,13 +727,13 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     const Shape fin = shape_of(smat);
     // strain_final (RadialShell.jl:736, guarded as ShellAnalysisGPU.jl:459)
     double sfin[6];
-    const double Frhoh = last.trace;
+    const double Frhoh = Lr[12];
     if (a.conv == HT_CONV_GPU && Frhoh == 0.0) {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) sfin[i] = last.k.E[i];
+        for (int i = 0; i < 6; ++i) sfin[i] = Lr[i];
     } else {
 #pragma unroll
-        for (int i = 0; i < 6; ++i) sfin[i] = last.k.E[i] * (Fbarx / Frhoh);
+        for (int i = 0; i < 6; ++i) sfin[i] = Lr[i] * (Fbarx / Frhoh);
     }
     // Sbar (RadialShell.jl:739-754) from the running sums at shell m0f - 1
     const double* qp = P + (size_t)(m0f - 1) * kRec;
@@ -884,7 +881,9 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
 
 template <bool PACKED>
 __global__ void __launch_bounds__(kThreads) walk_kernel(const WalkArgs a) {
+    extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
+    double* R = smem + (threadIdx.x >> 5) * kWarpSmemDoubles;
     const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const long long nw = (long long)gridDim.x * kWarpsPerBlock;
     double* P = a.scratch + gw * a.scratch_stride;
@@ -897,7 +896,7 @@ __global__ void __launch_bounds__(kThreads) walk_kernel(const WalkArgs a) {
         p = gw;
     }
     while (p < a.npeaks) {
-        process_peak<PACKED>(a, p, P, lane);
+        process_peak<PACKED>(a, p, P, R, lane);
         __syncwarp();
         if (a.dynamic) {
             int q = 0;
@@ -969,12 +968,22 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
                    int32_t nbuff, int8_t* d_mask, int32_t conv, int32_t mode,
                    const ht_results* out, cudaStream_t st) {
     const bool packed = mode == HT_MODE_BATCHED;
+    const size_t smem = (size_t)kWarpsPerBlock * kWarpSmemDoubles * sizeof(double);
     int bpsm = 0;
     cudaError_t e;
-    if (packed)
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<true>, kThreads, 0);
-    else
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<false>, kThreads, 0);
+    if (packed) {
+        e = cudaFuncSetAttribute(walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<true>, kThreads,
+                                                              smem);
+    } else {
+        e = cudaFuncSetAttribute(walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<false>, kThreads,
+                                                              smem);
+    }
     if (e != cudaSuccess) return ht_cuda_fail(e, "occupancy query");
     if (bpsm < 1) bpsm = 1;
     long long blocks = (long long)ctx->num_sms * bpsm;
@@ -1020,8 +1029,8 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st), "queue reset");
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_stats, 0, 2 * sizeof(unsigned long long), st),
                 "stats reset");
-    if (packed) walk_kernel<true><<<(unsigned)blocks, kThreads, 0, st>>>(a);
-    else walk_kernel<false><<<(unsigned)blocks, kThreads, 0, st>>>(a);
+    if (packed) walk_kernel<true><<<(unsigned)blocks, kThreads, smem, st>>>(a);
+    else walk_kernel<false><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch");
     ctx->last_kernels = 1;
     return HT_OK;

@@ -685,7 +685,13 @@ int or_analyse_peak(const or_grid* g, int64_t ipp, double alatt, int ir2min, dou
     double fcrit = fcrit_in >= 0.0 ? fcrit_in : or_fsc_of_z(ZZon - 1.0, ct);
     if (npart < 2) { set_no_collapse(out); return 4; }
 
-    int64_t maxm = npart + 2;
+    /* The reference sizes its profile arrays npart + 2 (RadialShell.jl:318); m never
+     * exceeds the number of distinct r^2 among the first npart cells, so that bound is
+     * used here (same values, smaller allocation). */
+    int64_t nsh_part = 1;
+    for (int64_t jp = 1; jp < npart; ++jp)
+        if (shells[jp].r2 != shells[jp - 1].r2) ++nsh_part;
+    int64_t maxm = nsh_part + 2;
     prof_t P;
     prof_alloc(&P, maxm);
     int64_t m = 1, m0 = 1;
