@@ -28,7 +28,7 @@ HT_MODE_BATCHED = 1
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
            "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_peakfind_filter", "ht_fields_pack",
-           "ht_shell_analyse", "ht_last_launch_stats")
+           "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats")
 
 
 class HTError(RuntimeError):
@@ -102,6 +102,9 @@ def load() -> C.CDLL:
     L.ht_shell_analyse.restype = C.c_int
     L.ht_shell_analyse.argtypes = [_P, C.POINTER(HtPeakBatch), dbl, dbl, i32, _P, i32, i32,
                                    C.POINTER(HtResults), _P]
+    L.ht_shell_analyse_static.restype = C.c_int
+    L.ht_shell_analyse_static.argtypes = [_P, C.POINTER(HtFields), C.POINTER(HtPeakBatch), dbl,
+                                          dbl, i32, _P, i32, C.POINTER(HtResults), _P]
     L.ht_last_launch_stats.restype = C.c_int
     L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
     _lib = L

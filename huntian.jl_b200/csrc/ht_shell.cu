@@ -17,6 +17,9 @@
 //           ht_pack_kernel, persistent grid with a dynamic work queue.
 #include <math.h>
 
+#include <mutex>
+#include <string>
+
 #include "ht_internal.cuh"
 
 namespace {
@@ -1032,6 +1035,125 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     if (packed) walk_kernel<true><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     else walk_kernel<false><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch");
+    ctx->last_kernels = 1;
+    return HT_OK;
+}
+
+// ------------------------------------------------- allocation-free entry point ----
+//
+// ht_shell_analyse_static: the shell collapse for callers that must not allocate device
+// memory during the call -- code running while a stream is being captured into a CUDA
+// graph, or hosts whose device memory is owned by a pool that only they may carve.  The
+// walk's per-warp profile scratch, which ht_shell_analyse sizes and allocates with
+// cudaMalloc, lives here in one file-scope __device__ array of kStaticScratchBytes
+// instead.  Every GPU that loads the library holds that array until the process exits.
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = 32u << 20;   // 32 MiB
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch per device, resolved once per device with that
+// device current (a host-side name of a __device__ array is not a device address).
+constexpr int kMaxDevices = 64;
+void* g_static_addr[kMaxDevices] = {};
+std::mutex g_static_mu;
+
+int static_scratch_address(int device, void** out) {
+    if (device < 0 || device >= kMaxDevices)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: device id out of range");
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return ht_cuda_fail(e, "cudaGetSymbolAddress(g_static_scratch)");
+        g_static_addr[device] = p;
+    }
+    *out = g_static_addr[device];
+    return HT_OK;
+}
+
+}  // namespace
+
+extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
+                                              const ht_peak_batch* b, double alatt,
+                                              double rmax2rs, int32_t nbuff, int8_t* d_mask,
+                                              int32_t conv, const ht_results* out,
+                                              void* stream) {
+    if (!ctx || !f || !b || !out)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: NULL argument");
+    if (!f->delta || !f->etax || !f->etay || !f->etaz)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: delta and eta x/y/z are required");
+    if ((f->eta2x || f->eta2y || f->eta2z) && !(f->eta2x && f->eta2y && f->eta2z))
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: give all of eta2x/y/z or none");
+    if (f->n1 < 1 || f->n1 != f->n2 || f->n1 != f->n3)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: the tile must be cubic");
+    if (b->npeaks < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: npeaks < 0");
+    if (b->npeaks > 0 && (!b->pi || !b->pj || !b->pk || !b->Rf || !b->ir2min || !b->ZZon ||
+                          !b->fcrit || !out->RTHL || !out->Fbarx || !out->e_v || !out->p_v ||
+                          !out->strain || !out->eigs || !out->Srb || !out->Sbar ||
+                          !out->Sbar2 || !out->gradpk || !out->gradpkf || !out->gradpkrf ||
+                          !out->d2F || !out->zvir_half))
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: NULL peak or result array");
+    if (!(alatt > 0.0)) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: alatt must be > 0");
+    if (conv != HT_CONV_GPU && conv != HT_CONV_CPU)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: unknown conv");
+    if (conv == HT_CONV_CPU && rmax2rs > 0.0)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: HT_CONV_CPU supports rmax2rs == 0 only");
+    if (nbuff < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: nbuff < 0");
+    if (ctx->nshells < 3)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: hunt radius too small");
+    // one 8-warp block must fit the static scratch
+    const long long stride = (long long)(ctx->nshells + 2) * kRec;
+    const size_t per_block = (size_t)kWarpsPerBlock * stride * sizeof(double);
+    if (per_block > kStaticScratchBytes)
+        return ht_fail(HT_ERR_CAPACITY,
+                       "ht_shell_analyse_static: the hunt radius needs " +
+                           std::to_string(per_block) + " bytes of scratch per block, more than "
+                           "the static maximum of " + std::to_string(kStaticScratchBytes));
+    ctx->last_kernels = 0;
+    if (b->npeaks == 0) return HT_OK;
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    void* scratch = nullptr;
+    int rc = static_scratch_address(ctx->device, &scratch);
+    if (rc != HT_OK) return rc;
+
+    const size_t smem = (size_t)kWarpsPerBlock * kWarpSmemDoubles * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(walk_kernel<false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return ht_cuda_fail(e, "cudaFuncSetAttribute");
+    int bpsm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<false>, kThreads, smem);
+    if (e != cudaSuccess) return ht_cuda_fail(e, "occupancy query");
+    long long blocks = (long long)ctx->num_sms * (bpsm > 0 ? bpsm : 1);
+    const long long fit = (long long)(kStaticScratchBytes / per_block);
+    const long long need = (b->npeaks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > fit) blocks = fit;
+    if (blocks > need) blocks = need;
+
+    WalkArgs a;
+    a.rec = nullptr;
+    a.delta = f->delta; a.ex = f->etax; a.ey = f->etay; a.ez = f->etaz;
+    a.e2x = f->eta2x; a.e2y = f->eta2y; a.e2z = f->eta2z; a.lapd = f->lapd;
+    a.n1 = f->n1; a.n2 = f->n2; a.n3 = f->n3;
+    a.s2 = (long long)f->n1 * f->n2;
+    a.off = ctx->d_off; a.start = ctx->d_start; a.count = ctx->d_count; a.r2 = ctx->d_r2;
+    a.rad = ctx->d_rad; a.nshells = ctx->nshells;
+    a.ct = ctx->d_ct; a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz;
+    a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
+    a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
+    a.pi = b->pi; a.pj = b->pj; a.pk = b->pk; a.Rf = b->Rf; a.ir2min = b->ir2min;
+    a.ZZon = b->ZZon; a.fcrit = b->fcrit; a.npeaks = b->npeaks;
+    a.alatt = alatt;
+    const double pi = 3.14159265358979323846;
+    a.aRnor = 3.0 / alatt;
+    a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
+    a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
+    a.scratch = (double*)scratch; a.scratch_stride = stride;
+    a.queue = nullptr; a.dynamic = 0;   // static peak-to-warp schedule: no counter to clear
+    a.stats = nullptr;
+    walk_kernel<false><<<(unsigned)blocks, kThreads, smem, (cudaStream_t)stream>>>(a);
+    HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch (static scratch)");
     ctx->last_kernels = 1;
     return HT_OK;
 }

@@ -165,6 +165,28 @@ class HaloFinder:
                                            C.byref(r), _stream_handle(stream)))
         return out
 
+    def analyse_static(self, fields: dict, pi, pj, pk, Rf, ir2min, ZZon, fcrit,
+                       alatt: float, *, rmax2rs: float = 0.0, nbuff: int = 0,
+                       mask: Optional[torch.Tensor] = None, conv: str = "gpu",
+                       out: dict, stream=None) -> dict:
+        """ht_shell_analyse_static: the same shell collapse with no device allocation in
+        the call (for code under stream capture or with a caller-owned memory pool).
+        `fields` maps delta, etax..etaz[, eta2x..eta2z, lapd] to device float32 tensors;
+        `out` must be preallocated (alloc_results).  The library's 32 MiB static scratch
+        is shared by all such calls: do not overlap them on the GPU."""
+        g = lambda k: fields.get(k)
+        n3, n2, n1 = fields["delta"].shape
+        f = HtFields(*[_ptr(g(k)) for k in ("delta", "etax", "etay", "etaz", "eta2x", "eta2y",
+                                             "eta2z", "lapd")], n1, n2, n3)
+        b = HtPeakBatch(pi.data_ptr(), pj.data_ptr(), pk.data_ptr(), Rf.data_ptr(),
+                        ir2min.data_ptr(), ZZon.data_ptr(), fcrit.data_ptr(), int(pi.numel()))
+        r = HtResults(*[out[n].data_ptr() for n in RESULT_NAMES])
+        check(_lib.load().ht_shell_analyse_static(self._h, C.byref(f), C.byref(b), float(alatt),
+                                                  float(rmax2rs), int(nbuff), _ptr(mask),
+                                                  _CONV[conv], C.byref(r),
+                                                  _stream_handle(stream)))
+        return out
+
     def last_stats(self):
         k, s, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(_lib.load().ht_last_launch_stats(self._h, C.byref(k), C.byref(s), C.byref(c)))

@@ -180,6 +180,31 @@ HT_API int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* batch, double alat
                      double rmax2rs, int32_t nbuff, int8_t* d_mask, int32_t conv,
                      int32_t mode, const ht_results* out, void* stream);
 
+/* Allocation-free variant of ht_shell_analyse.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc while they run this step: code issuing work
+ * into a stream that is being captured into a CUDA graph (allocation is not a capturable
+ * operation), or hosts whose device memory belongs to a pool they manage themselves.
+ * The call allocates nothing: the shell walk's per-warp scratch is a 32 MiB file-scope
+ * __device__ array inside the library (held by every GPU that loads the library until
+ * the process exits), and the fields are read in place (no interleaved-record copy, no
+ * ht_fields_pack needed).  The caller passes the tile, the peaks and the result arrays;
+ * `ctx` (created beforehand) supplies the shell and collapse tables.  Results equal
+ * ht_shell_analyse's.
+ *
+ * - The first call on a device resolves the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call before any
+ *   stream capture begins.
+ * - All calls share the one array: calls whose kernels overlap on the GPU (e.g. on two
+ *   streams, or from two threads) race on it and give wrong results.  Serialize them.
+ * - Limit: the hunt radius must leave one 8-warp block's scratch,
+ *   8 * (nshells + 2) * 192 bytes, within 32 MiB (always true for nhunt <= 127);
+ *   otherwise HT_ERR_CAPACITY.  Larger hunt radii run fewer concurrent warps. */
+HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
+                                   const ht_peak_batch* batch, double alatt, double rmax2rs,
+                                   int32_t nbuff, int8_t* d_mask, int32_t conv,
+                                   const ht_results* out, void* stream);
+
 /* Launch statistics of the last ht_shell_analyse on this context: kernels launched and
  * the total number of shells walked (for the roofline's algorithmic bytes). */
 HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
