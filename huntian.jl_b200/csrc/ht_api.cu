@@ -121,6 +121,76 @@ static void build_akk(std::vector<double>& akk) {
     akk[1100] = 0.0;
 }
 
+// hRinteg (RadialShell.jl:95-121): integral of the SPH kernel 4 pi W(x) x (x^2 - u12)
+// from |u0| to 2 (Fortran peakvoidsubs.f90 hRinteg).
+static double hRinteg(double u0, double u12) {
+    const double x0 = fabs(u0);
+    if (x0 >= 2.0) return 0.0;
+    const double one7 = 1.0 / 7.0;
+    double result = 1.6 * u12 - 6.4 * one7;
+    const double x02 = x0 * x0, x04 = x02 * x02;
+    if (x0 >= 1.0) {
+        const double h1 = x04 * (2.0 - x0 * (2.4 - x0 * (1.0 - x0 * one7)));
+        const double h2 = x02 * (4.0 - x0 * (4.0 - x0 * (1.5 - x0 * 0.2)));
+        result = result - h2 * u12 + h1;
+    } else {
+        result = result - 0.2 * (u12 - one7);
+        if (x0 > 0.0) {
+            const double h1 = x04 * (1.0 - x02 * (1.0 - 3.0 * x0 * one7));
+            const double h2 = x02 * (2.0 - x02 * (1.5 - 0.6 * x0));
+            result = result - h2 * u12 + h1;
+        }
+    }
+    return result;
+}
+
+// Weight table of kernel_strain (RadialShell.jl:225-274, hlatt = 1).  Row mp > 1: the
+// shells m1 >= 2 with u0^2 < 4, u0 = rad[mp] - rad[m1], weight
+// hRinteg(u0, u12) / (u12 - u0^2)^2 with u12 = rad[mp]^2 + rad[m1]^2.  Row 1 (the central
+// branch, used by the inward walk's last step, whose window is shells 2..U(1) with
+// U(1) the last shell below radius 2): weight 0.5 * akk(100 rad^2) / rad[m1] with akk
+// linearly interpolated.  These are the reference's weights, evaluated once.
+static void build_weights(const std::vector<double>& rad, int nshells,
+                          const std::vector<double>& akk, std::vector<int32_t>& row,
+                          std::vector<int32_t>& m1s, std::vector<double>& wts) {
+    row.assign((size_t)nshells + 2, 0);
+    m1s.clear();
+    wts.clear();
+    int lo = 2;
+    for (int mp = 1; mp <= nshells; ++mp) {
+        row[mp] = (int32_t)m1s.size();
+        if (mp == 1) {
+            for (int m1 = 2; m1 <= nshells && rad[m1] < 2.0; ++m1) {
+                const double r1 = rad[m1];
+                const double con = 100.0 * r1 * r1;
+                const double fl = floor(con);
+                const int icon = (int)fl;
+                const double diff = con - fl;
+                double aww = 0.0;
+                if (icon >= 0 && icon < 1100) aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
+                m1s.push_back(m1);
+                wts.push_back(0.5 * aww / r1);
+            }
+            continue;
+        }
+        const double rmp = rad[mp];
+        while (lo < mp && (rmp - rad[lo]) * (rmp - rad[lo]) >= 4.0) ++lo;
+        for (int m1 = lo; m1 <= nshells; ++m1) {
+            const double u0 = rmp - rad[m1];
+            const double u02 = u0 * u0;
+            if (!(u02 < 4.0)) {
+                if (m1 > mp) break;
+                continue;
+            }
+            const double u12 = rmp * rmp + rad[m1] * rad[m1];
+            const double den = u12 - u02;
+            m1s.push_back(m1);
+            wts.push_back(hRinteg(u0, u12) / (den * den));
+        }
+    }
+    row[(size_t)nshells + 1] = (int32_t)m1s.size();
+}
+
 // Trilinear lookup on the host copy (CollapseTable.jl:126-138), for fsc_of_z.
 static double host_interp(const ht_ctx* c, double x, double y, double z) {
     if (!(x >= c->X1 && x <= c->X2 && y >= c->Y1 && y <= c->Y2 && z >= c->Z1 && z <= c->Z2))
@@ -145,6 +215,7 @@ static double host_interp(const ht_ctx* c, double x, double y, double z) {
 
 static void free_ctx(ht_ctx* c) {
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
+                    c->d_wrow, c->d_wm1, c->d_wwt,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_queue, c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -188,6 +259,11 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
     c->out_val = out_val;
     std::vector<double> akk;
     build_akk(akk);
+    std::vector<int32_t> wrow, wm1;
+    std::vector<double> wwt;
+    build_weights(rad, c->nshells, akk, wrow, wm1, wwt);
+    c->nweights = (int64_t)wm1.size();
+    if (const char* v = getenv("HT_SMALL_MAX_SHELLS")) c->small_max_shells = atoi(v);
     int rc;
     if ((rc = upload(&c->d_off, c->h_off.data(), c->h_off.size(), "shell offsets")) ||
         (rc = upload(&c->d_start, c->h_start.data(), c->h_start.size(), "shell starts")) ||
@@ -196,6 +272,9 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
         (rc = upload(&c->d_rad, rad.data(), rad.size(), "shell radii")) ||
         (rc = upload(&c->d_ct, c->h_ct.data(), c->h_ct.size(), "collapse table")) ||
         (rc = upload(&c->d_akk, akk.data(), akk.size(), "SPH table")) ||
+        (rc = upload(&c->d_wrow, wrow.data(), wrow.size(), "weight rows")) ||
+        (rc = upload(&c->d_wm1, wm1.data(), wm1.size(), "weight shells")) ||
+        (rc = upload(&c->d_wwt, wwt.data(), wwt.size(), "weights")) ||
         (rc = ht_alloc((void**)&c->d_queue, 256, "work queue")) ||
         (rc = ht_alloc((void**)&c->d_stats, 256, "launch stats"))) {
         free_ctx(c);

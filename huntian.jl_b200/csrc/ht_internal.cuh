@@ -27,6 +27,14 @@ struct ht_ctx {
     int32_t* d_count = nullptr;    // [nshells + 2]
     int32_t* d_r2 = nullptr;       // [nshells + 2]
     double* d_rad = nullptr;       // sqrt(r2), [nshells + 2]
+    // SPH window weights of kernel_strain (RadialShell.jl:225-274), which depend only on
+    // the two shell radii: row mp holds entries [wrow[mp], wrow[mp+1]) of (m1, weight)
+    int64_t nweights = 0;
+    int32_t* d_wrow = nullptr;     // [nshells + 2]
+    int32_t* d_wm1 = nullptr;
+    double* d_wwt = nullptr;
+    // peaks whose minimum walk spans at most this many shells run 8 lanes per peak
+    int small_max_shells = 96;
 
     // collapse table + SPH table
     std::vector<float> h_ct;

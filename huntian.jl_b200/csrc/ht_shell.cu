@@ -1,20 +1,26 @@
-// Radial-shell collapse on sm_100a: one warp per peak.
+// Radial-shell collapse on sm_100a.
 //
-// For every peak the warp walks the shells of the r^2-sorted offset table outward
-// (the per-shell gather of ShellAnalysisGPU.jl:153-229 / ext/CUDAExt.jl:752-924),
-// accumulating 22 FP32 sums per shell with Kahan compensation in each lane and
-// combining the lanes in FP64.  The per-shell profile (Fbar, gradients, symmetrised
-// strain sums and running means) goes to a per-warp scratch slot in FP64.  The walk
-// stops as soon as every shell the post-processing can read has been gathered.  The
-// same warp then runs the post-processing of RadialShell.jl:449-859 /
-// ext/CUDAExt.jl:1213-1912 in FP64: fcrit crossing, the inward strain/eigen/barrier
-// walk (32 steps evaluated at once, one per lane), RTHL interpolation, Sbar, Srb, d2F,
-// zvir_half and the mask update.
+// A peak is handled by a group of G lanes of one warp: G = 8 for peaks whose walk is
+// short (four peaks share a warp), G = 32 for the rest.  G is a pure function of the
+// peak's own filter radius and ir2min, so every execution mode gives bit-identical
+// results.  For each peak the group walks the shells of the r^2-sorted offset table
+// outward (the per-shell gather of ShellAnalysisGPU.jl:153-229 / ext/CUDAExt.jl:752-924):
+// each lane accumulates 13 FP32 sums per shell with Kahan compensation (delta, delta*d,
+// delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L), the lanes' partial sums
+// are combined in FP64 in a fixed order through shared memory, and the shell's profile
+// (Fbar, gradients, strain) goes to a per-group scratch slot in FP64.  The walk stops as
+// soon as every shell the post-processing reads has been gathered.  The same group then
+// runs the post-processing of RadialShell.jl:449-859 / ext/CUDAExt.jl:1213-1912 in FP64:
+// fcrit crossing, the inward strain/eigen/barrier walk (G steps evaluated at once, one per
+// lane), RTHL interpolation, Sbar (a second pass over the cells within the collapsed
+// radius), Srb, d2F, zvir_half and the mask update.  The SPH window weights of
+// kernel_strain depend only on the two shell radii, so they come from a table built once
+// per context.
 //
 // Two execution modes give identical results:
-//   PLAIN   reads the eight reference fields separately, static peak->warp schedule;
+//   PLAIN   reads the eight reference fields separately, static item->warp schedule;
 //   BATCHED reads 32-byte interleaved cell records (one sector per cell) built by
-//           ht_pack_kernel, persistent grid with a dynamic work queue.
+//           pack_kernel, persistent grid with a dynamic work queue.
 #include <math.h>
 
 #include <mutex>
@@ -26,7 +32,9 @@ namespace {
 
 constexpr int kWarpsPerBlock = 8;
 constexpr int kThreads = kWarpsPerBlock * 32;
-constexpr int kRec = 24;   // doubles per shell in the scratch profile
+constexpr int kRec = 16;          // doubles per shell in the scratch profile
+constexpr int kPeaksPerItem = 4;  // consecutive peaks per work item
+constexpr int kSmallG = 8;        // lanes per peak for short walks
 
 // Scratch profile record, one per shell m (1-based):
 enum : int {
@@ -34,16 +42,22 @@ enum : int {
     P_G = 1,      // 3: Gshell / rad
     P_GF = 4,     // 3: Gshellf / rad
     P_SR = 7,     // 6: (SR_LK + SR_KL) / rad for 11, 22, 33, 12, 13, 23
-    P_CS = 13,    // 3: running sum of Sshell over shells 1..m
-    P_CS2 = 16,   // 3: running sum of S2shell
-    P_CN = 19,    // running count of in-tile cells
-    P_CSRB = 20,  // running Srb numerator, RadialShell.jl:760-764
+    P_CSRB = 13,  // running Srb numerator, RadialShell.jl:760-764
 };
 
-// Values held by the lanes after the transposed reduction of one shell.
-enum : int {
-    V_F = 0, V_N = 1, V_S = 2, V_S2 = 5, V_G = 8, V_GF = 11, V_SR = 14, V_COUNT = 23
-};
+// Per-cell sums gathered for every shell.
+enum : int { V_F = 0, V_N = 1, V_G = 2, V_GF = 5, V_SR = 8, V_ROWS = 14 };
+
+// Shared-memory staging per group: [V_ROWS][G + 1] doubles for the shell sums (the last
+// column holds the totals), or [G + 1][kStepW] doubles for inward-walk steps.
+constexpr int kStepW = 16;
+__host__ __device__ constexpr int group_smem_doubles(int G) {
+    return V_ROWS * (G + 1) > (G + 1) * kStepW ? V_ROWS * (G + 1) : (G + 1) * kStepW;
+}
+constexpr int kWarpSmemDoubles =
+    group_smem_doubles(32) > (32 / kSmallG) * group_smem_doubles(kSmallG)
+        ? group_smem_doubles(32)
+        : (32 / kSmallG) * group_smem_doubles(kSmallG);
 
 struct WalkArgs {
     const float4* rec;
@@ -64,6 +78,9 @@ struct WalkArgs {
     const int32_t* r2;
     const double* rad;
     int nshells;
+    const int32_t* wrow;   // SPH weight table: row mp = entries [wrow[mp], wrow[mp+1])
+    const int32_t* wm1;
+    const double* wwt;
 
     const float* ct;
     int nx, ny, nz;
@@ -82,10 +99,11 @@ struct WalkArgs {
     double alatt, wRnor, aRnor, rmax2rs;
     int nbuff;
     int conv;
+    int small_max_shells;   // peaks whose minimum walk is <= this use G = 8
     int8_t* mask;
     ht_results out;
 
-    double* scratch;
+    double* scratch;        // one slot of scratch_stride doubles per group
     long long scratch_stride;
     int32_t* queue;
     int dynamic;
@@ -136,27 +154,23 @@ __device__ __forceinline__ int first_above(const double* rad, int lo, int hi, do
     return ans;
 }
 
-// RadialShell.jl:95-121 (Fortran hRinteg).
-__device__ __forceinline__ double hRinteg(double u0, double u12) {
-    double x0 = fabs(u0);
-    if (x0 >= 2.0) return 0.0;
-    const double one7 = 1.0 / 7.0;
-    double result = 1.6 * u12 - 6.4 * one7;
-    double x02 = x0 * x0, x04 = x02 * x02;
-    if (x0 >= 1.0) {
-        double h1 = x04 * (2.0 - x0 * (2.4 - x0 * (1.0 - x0 * one7)));
-        double h2 = x02 * (4.0 - x0 * (4.0 - x0 * (1.5 - x0 * 0.2)));
-        result = result - h2 * u12 + h1;
-    } else {
-        result = result - 0.2 * (u12 - one7);
-        if (x0 > 0.0) {
-            double h1 = x04 * (1.0 - x02 * (1.0 - 3.0 * x0 * one7));
-            double h2 = x02 * (2.0 - x02 * (1.5 - 0.6 * x0));
-            result = result - h2 * u12 + h1;
-        }
+// G lanes of one warp working on one peak.
+struct Group {
+    int G, t, q;
+    unsigned mask;
+    __device__ __forceinline__ double shfl(double v, int src) const {
+        return __shfl_sync(mask, v, src, G);
     }
-    return result;
-}
+    __device__ __forceinline__ unsigned ballot(bool p) const {
+        const unsigned b = __ballot_sync(mask, p) >> (q * G);
+        return G == 32 ? b : (b & ((1u << G) - 1u));
+    }
+    __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+    __device__ __forceinline__ double sum(double x) const {
+        for (int o = G >> 1; o >= 1; o >>= 1) x += __shfl_xor_sync(mask, x, o, G);
+        return x;
+    }
+};
 
 struct Strain {
     double E[6];   // 11, 22, 33, 12, 13, 23
@@ -164,61 +178,36 @@ struct Strain {
     double gf[3];
 };
 
-// kernel_strain (RadialShell.jl:225-274) over shells lo..hi of the profile `P`,
-// centred on shell mp, in FP64.  Shells at |rad[mp] - rad[m1]| >= 2 carry no weight.
-__device__ Strain kernel_strain(const double* __restrict__ P, const double* __restrict__ rad,
-                                const double* __restrict__ akk, int mp, int lo, int hi,
-                                double wRnor, double aRnor) {
+// kernel_strain (RadialShell.jl:225-274) centred on shell mp over the shells m1 of its
+// weight-table row with lo <= m1 <= hi, in FP64.  The row of mp > 1 lists the shells
+// with (rad[mp] - rad[m1])^2 < 4 and hRinteg(u0, u12) / (u12 - u0^2)^2 as weight; the
+// row of mp = 1 lists shells 2..U(1) with the atab4 weight 0.5 * W / rad[m1].  The
+// weighted sums are scaled by wRnor / rad[mp] (mp > 1) or aRnor (mp = 1) at the end, in
+// the reference's order.
+__device__ __noinline__ Strain kernel_strain(const WalkArgs& a, const double* __restrict__ P,
+                                             int mp, int lo, int hi) {
     Strain s;
 #pragma unroll
     for (int i = 0; i < 6; ++i) s.E[i] = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) { s.g[i] = 0.0; s.gf[i] = 0.0; }
-    double scale;
-    if (mp > 1) {
-        const double rmp = rad[mp];
-        for (int m1 = lo; m1 <= hi; ++m1) {
-            const double r1 = rad[m1];
-            const double u0 = rmp - r1;
-            const double u02 = u0 * u0;
-            if (u02 < 4.0) {
-                const double u12 = rmp * rmp + r1 * r1;
-                const double den = u12 - u02;
-                const double wt = hRinteg(u0, u12) / (den * den);
-                const double* q = P + (size_t)m1 * kRec;
-                const double hw = 0.5 * wt;
+    const int e0 = __ldg(a.wrow + mp), e1 = __ldg(a.wrow + mp + 1);
+    for (int e = e0; e < e1; ++e) {
+        const int m1 = __ldg(a.wm1 + e);
+        if (m1 > hi) break;
+        if (m1 < lo) continue;
+        const double wt = __ldg(a.wwt + e);
+        const double hw = 0.5 * wt;
+        const double* q = P + (size_t)m1 * kRec;
 #pragma unroll
-                for (int L = 0; L < 3; ++L) {
-                    s.g[L] += wt * q[P_G + L];
-                    s.gf[L] += wt * q[P_GF + L];
-                }
-#pragma unroll
-                for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
-            }
+        for (int L = 0; L < 3; ++L) {
+            s.g[L] += wt * q[P_G + L];
+            s.gf[L] += wt * q[P_GF + L];
         }
-        scale = wRnor / rmp;
-    } else {
-        for (int m1 = lo; m1 <= hi; ++m1) {
-            const double r1 = rad[m1];
-            const double con = 100.0 * r1 * r1;
-            const double fl = floor(con);
-            const int icon = (int)fl;
-            const double diff = con - fl;
-            double aww = 0.0;
-            if (icon >= 0 && icon < 1100) aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
-            const double wt = 0.5 * aww / r1;
-            const double* q = P + (size_t)m1 * kRec;
-            const double hw = 0.5 * wt;
 #pragma unroll
-            for (int L = 0; L < 3; ++L) {
-                s.g[L] += wt * q[P_G + L];
-                s.gf[L] += wt * q[P_GF + L];
-            }
-#pragma unroll
-            for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
-        }
-        scale = aRnor;
+        for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
     }
+    const double scale = mp > 1 ? a.wRnor / a.rad[mp] : a.aRnor;
 #pragma unroll
     for (int i = 0; i < 6; ++i) s.E[i] *= scale;
 #pragma unroll
@@ -226,10 +215,47 @@ __device__ Strain kernel_strain(const double* __restrict__ P, const double* __re
     return s;
 }
 
+// kernel_strain's central branch over shells lo..hi computed directly (used for the
+// gradient at the filter scale when mrf = 1, whose window starts at the centre shell:
+// its weight 0.5 * W(0) / 0 is infinite and the reference's gradient is NaN).
+__device__ __noinline__ Strain kernel_strain_central(const WalkArgs& a,
+                                                     const double* __restrict__ P, int lo,
+                                                     int hi) {
+    Strain s;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s.E[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { s.g[i] = 0.0; s.gf[i] = 0.0; }
+    for (int m1 = lo; m1 <= hi; ++m1) {
+        const double r1 = a.rad[m1];
+        const double con = 100.0 * r1 * r1;
+        const double fl = floor(con);
+        const int icon = (int)fl;
+        const double diff = con - fl;
+        double aww = 0.0;
+        if (icon >= 0 && icon < 1100) aww = a.akk[icon] + diff * (a.akk[icon + 1] - a.akk[icon]);
+        const double wt = 0.5 * aww / r1;
+        const double hw = 0.5 * wt;
+        const double* q = P + (size_t)m1 * kRec;
+#pragma unroll
+        for (int L = 0; L < 3; ++L) {
+            s.g[L] += wt * q[P_G + L];
+            s.gf[L] += wt * q[P_GF + L];
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
+    }
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s.E[i] *= a.aRnor;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { s.g[i] *= a.aRnor; s.gf[i] *= a.aRnor; }
+    return s;
+}
+
 // Ascending eigenvalues of a symmetric 3x3 matrix by cyclic Jacobi rotations in FP64
 // (Golub & Van Loan, Alg. 8.4.3), replacing LAPACK eigvals(Symmetric)
 // (RadialShell.jl:215-220).  E = (11, 22, 33, 12, 13, 23).
-__device__ void eig3(const double E[6], double lam[3]) {
+__device__ __noinline__ void eig3(const double* E, double* lam) {
     double a[3][3];
     a[0][0] = E[0]; a[1][1] = E[1]; a[2][2] = E[2];
     a[0][1] = a[1][0] = E[3];
@@ -272,7 +298,7 @@ __device__ void eig3(const double E[6], double lam[3]) {
 
 // Trilinear collapse-table lookup, -1 (out_val) outside the closed box
 // (CollapseTable.jl:126-138), in FP64 over the Float32 table.
-__device__ double interp3(const WalkArgs& a, double x, double y, double z) {
+__device__ __noinline__ double interp3(const WalkArgs& a, double x, double y, double z) {
     if (!(x >= a.X1 && x <= a.X2 && y >= a.Y1 && y <= a.Y2 && z >= a.Z1 && z <= a.Z2))
         return a.out_val;
     double tx = (x - a.X1) / ((a.X2 - a.X1) / (a.nx - 1));
@@ -311,79 +337,43 @@ __device__ __forceinline__ Shape shape_of(const double E[6]) {
     return s;
 }
 
-// Per-warp shared-memory staging: the 23 per-lane shell sums during the walk, and the
-// results of 32 inward-walk steps (+ one carried step) during the post-processing.
-constexpr int kRedRows = 23, kRedPitch = 33;          // [value][lane], padded pitch
-constexpr int kStepW = 16, kStepRows = 33;            // [lane or carry][field]
-constexpr int kWarpSmemDoubles =
-    kRedRows * kRedPitch > kStepRows * kStepW ? kRedRows * kRedPitch : kStepRows * kStepW;
-
-// Lane v (< 23) returns the warp total of value v, summed over lanes 0..31 in order
-// (deterministic).  `R` is the warp's staging area.
-__device__ __forceinline__ double warp_column_sum(double* R, int lane) {
-    __syncwarp();
-    double s = 0.0;
-    if (lane < kRedRows) {
-        const double* r = R + lane * kRedPitch;
-#pragma unroll 8
-        for (int t = 0; t < 32; ++t) s += r[t];
-    }
-    __syncwarp();
-    return s;
-}
-
-__device__ __forceinline__ double warp_sum(double x) {
-#pragma unroll
-    for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    return x;
-}
-
-__device__ void write_no_collapse(const WalkArgs& a, long long p, int lane) {
-    const ht_results& o = a.out;
-    if (lane == 0) {
-        o.RTHL[p] = -1.0f; o.Fbarx[p] = 0.f; o.e_v[p] = 0.f; o.p_v[p] = 0.f;
-        o.Srb[p] = 0.f; o.d2F[p] = 0.f; o.zvir_half[p] = -1.0f;
-    }
-    if (lane < 9) o.strain[9 * p + lane] = 0.f;
-    if (lane < 3) {
-        o.eigs[3 * p + lane] = 0.f; o.Sbar[3 * p + lane] = 0.f; o.Sbar2[3 * p + lane] = 0.f;
-        o.gradpk[3 * p + lane] = 0.f; o.gradpkf[3 * p + lane] = 0.f;
-        o.gradpkrf[3 * p + lane] = 0.f;
-    }
-}
-
-// One step of the inward walk evaluated by one lane.
+// zvir of one inward-walk step (RadialShell.jl:629-648): the step's strain, its
+// eigen trace (Frhoh) and zvir at shell mp.
 struct Step {
     Strain k;
-    double trace;   // Frhoh
+    double trace;
     double zvir;
 };
 
 __device__ __forceinline__ Step eval_step(const WalkArgs& a, const double* P, int mp, int m,
                                           bool force_minus_one) {
-    const double* rad = a.rad;
-    int lo, hi;
-    if (mp > 1) {
-        lo = first_above(rad, 2, mp, fmax(rad[mp] - 2.0, 0.0));
-        hi = last_below(rad, mp, m, rad[mp] + 2.0);
-        if (hi < mp) hi = mp;
-    } else {
-        lo = 2;
-        hi = last_below(rad, 2, m, 2.0);
-    }
     Step st;
-    st.k = kernel_strain(P, rad, a.akk, mp, lo, hi, a.wRnor, a.aRnor);
-    Shape sh = shape_of(st.k.E);
+    st.k = kernel_strain(a, P, mp, 1, m);
+    const Shape sh = shape_of(st.k.E);
     st.trace = sh.trace;
     st.zvir = -1.0;
     if (!force_minus_one) {
         const double Frho = P[(size_t)mp * kRec + P_FBAR];
         if (Frho > 0.0) {
-            double poe = sh.e_v < 1e-5 ? 0.0 : sh.p_v / sh.e_v;
+            const double poe = sh.e_v < 1e-5 ? 0.0 : sh.p_v / sh.e_v;
             st.zvir = interp3(a, log10(Frho), sh.e_v, poe);
         }
     }
     return st;
+}
+
+__device__ void write_no_collapse(const WalkArgs& a, long long p, const Group& g) {
+    const ht_results& o = a.out;
+    for (int i = g.t; i < 9; i += g.G) o.strain[9 * p + i] = 0.f;
+    if (g.t < 3) {
+        o.eigs[3 * p + g.t] = 0.f; o.Sbar[3 * p + g.t] = 0.f; o.Sbar2[3 * p + g.t] = 0.f;
+        o.gradpk[3 * p + g.t] = 0.f; o.gradpkf[3 * p + g.t] = 0.f;
+        o.gradpkrf[3 * p + g.t] = 0.f;
+    }
+    if (g.t == 0) {
+        o.RTHL[p] = -1.0f; o.Fbarx[p] = 0.f; o.e_v[p] = 0.f; o.p_v[p] = 0.f;
+        o.Srb[p] = 0.f; o.d2F[p] = 0.f; o.zvir_half[p] = -1.0f;
+    }
 }
 
 template <bool PACKED>
@@ -391,10 +381,8 @@ struct CellLoader;
 
 template <>
 struct CellLoader<true> {
-    __device__ __forceinline__ static void load(const WalkArgs& a, int iv1, int iv2, int iv3,
-                                                float (&v)[8]) {
-        const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
-                              a.s2 * (iv3 - 1);
+    __device__ __forceinline__ static void load(const WalkArgs& a, long long idx, int iv1,
+                                                int iv2, int iv3, float (&v)[8]) {
         const float4 x = __ldg(a.rec + 2 * idx);
         const float4 y = __ldg(a.rec + 2 * idx + 1);
         v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
@@ -404,10 +392,8 @@ struct CellLoader<true> {
 
 template <>
 struct CellLoader<false> {
-    __device__ __forceinline__ static void load(const WalkArgs& a, int iv1, int iv2, int iv3,
-                                                float (&v)[8]) {
-        const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
-                              a.s2 * (iv3 - 1);
+    __device__ __forceinline__ static void load(const WalkArgs& a, long long idx, int iv1,
+                                                int iv2, int iv3, float (&v)[8]) {
         // transposed read delta[iv3, iv1, iv2] (ext/CUDAExt.jl:819-820), cubic tile
         const long long idt = (long long)(iv3 - 1) + (long long)a.n1 * (iv1 - 1) +
                               a.s2 * (iv2 - 1);
@@ -428,7 +414,6 @@ struct CellLoader<false> {
 // CPU convention, ShellAnalysisGPU.jl:234-254 for the GPU one): the first shell s >= 2
 // minimising |r2[s] - (Rf/alatt)^2| below 10, minus the lag of the reference counters.
 __device__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
-    // first s in [2, smax] with r2 >= R2
     int lo = 2, hi = smax, first_ge = smax + 1;
     while (lo <= hi) {
         int mid = (lo + hi) >> 1;
@@ -436,7 +421,6 @@ __device__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
     }
     int best = -1;
     double bestd = 10.0;
-    // candidates in ascending order: first_ge - 1, first_ge (strict < keeps the first)
     for (int s = max(2, first_ge - 1); s <= min(smax, first_ge); ++s) {
         double d = fabs((double)a.r2[s] - R2);
         if (d < bestd) { bestd = d; best = s; }
@@ -446,219 +430,193 @@ __device__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
     return best >= 3 ? best - 2 : 1;
 }
 
+// Data-independent walk bounds of a peak: the last finalised shell m, the first shell
+// past ir2min (m0_init), mrf and the last shell of mrf's window (need_rf).
+struct Bounds { int m, m0_init, mrf, need_rf; };
+
+__device__ __forceinline__ Bounds peak_bounds(const WalkArgs& a, double Rf, int ir2min) {
+    Bounds b;
+    const int nshells = a.nshells;
+    // nshells - 1: the reference's per-cell loop never closes the last shell; rmax2rs
+    // limits the shells further (ext/CUDAExt.jl:2192-2200)
+    b.m = nshells - 1;
+    if (a.rmax2rs > 0.0) {
+        const double lim = a.rmax2rs * Rf / a.alatt;
+        const double r2lim = lim * lim;
+        int lo = 1, hi = nshells - 1, cnt = 0;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            if ((double)a.r2[mid] <= r2lim) { cnt = mid; lo = mid + 1; } else { hi = mid - 1; }
+        }
+        b.m = cnt;
+    }
+    b.m0_init = b.m;
+    {
+        int lo = 2, hi = b.m;
+        while (lo <= hi) {
+            int mid = (lo + hi) >> 1;
+            if (a.r2[mid] > ir2min) { b.m0_init = mid; hi = mid - 1; } else { lo = mid + 1; }
+        }
+    }
+    const double RR = Rf / a.alatt;
+    b.mrf = b.m >= 2 ? find_mrf(a, RR * RR, a.conv == HT_CONV_GPU ? b.m : nshells, a.conv) : 1;
+    b.need_rf = b.m >= 2 ? max(b.mrf, last_below(a.rad, 1, b.m, a.rad[b.mrf] + 2.0)) : 1;
+    return b;
+}
+
+// G = 8 for peaks whose data-independent minimum walk (to the first shell past ir2min
+// and the window of mrf) has at most small_max_shells shells, else 32.
+__device__ __forceinline__ int group_size(const WalkArgs& a, long long p) {
+    const Bounds b = peak_bounds(a, a.Rf[p], a.ir2min[p]);
+    return max(b.m0_init, b.need_rf) <= a.small_max_shells ? kSmallG : 32;
+}
+
 template <bool PACKED>
 __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P,
-                             double* __restrict__ R, int lane) {
+                             double* __restrict__ R, const Group& g) {
     const double* rad = a.rad;
+    const int G = g.G, t = g.t, RP = G + 1;
     const int ci = a.pi[p], cj = a.pj[p], ck = a.pk[p];
     const double Rf = a.Rf[p];
     const int ir2min = a.ir2min[p];
     const double ZZon = (double)a.ZZon[p];
     const double fcrit = (double)a.fcrit[p];
-    const int nshells = a.nshells;
     if (ci < 1 || ci > a.n1 || cj < 1 || cj > a.n2 || ck < 1 || ck > a.n3) {
         // a centre outside the tile has no cells to walk (the reference would fault)
-        write_no_collapse(a, p, lane);
+        write_no_collapse(a, p, g);
         return;
     }
-
-    // last shell that is finalised (nshells - 1: the reference's per-cell loop never
-    // closes the last shell), optionally limited by rmax2rs (ext/CUDAExt.jl:2192-2200)
-    int m = nshells - 1;
-    if (a.rmax2rs > 0.0) {
-        const double lim = a.rmax2rs * Rf / a.alatt;
-        const double r2lim = lim * lim;
-        int cnt = 0;
-        for (int s = 1; s <= nshells - 1; ++s) {
-            if (!((double)a.r2[s] <= r2lim)) break;
-            cnt = s;
-        }
-        m = cnt;
-    }
-    if (m < 2) { write_no_collapse(a, p, lane); return; }
-
-    // data-independent shell indices
-    int m0_init = m;
-    {
-        int lo = 2, hi = m;
-        while (lo <= hi) {
-            int mid = (lo + hi) >> 1;
-            if (a.r2[mid] > ir2min) { m0_init = mid; hi = mid - 1; } else { lo = mid + 1; }
-        }
-    }
-    const double RR = Rf / a.alatt;
-    const int mrf = find_mrf(a, RR * RR, a.conv == HT_CONV_GPU ? m : nshells, a.conv);
-    const int need_rf = max(mrf, last_below(rad, 1, m, rad[mrf] + 2.0));
+    const Bounds bd = peak_bounds(a, Rf, ir2min);
+    const int m = bd.m;
+    if (m < 2) { write_no_collapse(a, p, g); return; }
 
     // ---------------------------------------------------------------- walk ----
-    // centre cell (shell 1)
     float cv[8];
-    CellLoader<PACKED>::load(a, ci, cj, ck, cv);
+    const long long cidx = (long long)(ci - 1) + (long long)a.n1 * (cj - 1) + a.s2 * (ck - 1);
+    CellLoader<PACKED>::load(a, cidx, ci, cj, ck, cv);
     const double Fbar1 = (double)cv[0];
-    {
-        double* q = P + kRec;
-        if (lane < kRec) {
-            double v = 0.0;
-            if (lane == P_FBAR) v = Fbar1;
-            else if (lane >= P_CS && lane < P_CS + 3) v = (double)cv[2 + lane - P_CS];
-            else if (lane >= P_CS2 && lane < P_CS2 + 3) v = (double)cv[5 + lane - P_CS2];
-            else if (lane == P_CN) v = 1.0;
-            q[lane] = v;
-        }
-    }
+    for (int i = t; i < kRec; i += G) P[kRec + i] = i == P_FBAR ? Fbar1 : 0.0;
     double Fbarp = Fbar1, dFbarp = Fbar1, radp = 0.0, rad5p = 0.0, csrb = 0.0;
-    // running sums held by the lane that owns the value after the reduction
-    double cum = 0.0;
-    if (lane >= V_S && lane < V_S + 3) cum = (double)cv[2 + lane - V_S];
-    if (lane >= V_S2 && lane < V_S2 + 3) cum = (double)cv[5 + lane - V_S2];
-    if (lane == V_N) cum = 1.0;
-
     int m_c = 0;          // first shell >= m0_init with Fbar < fcrit (0: none yet)
-    int stop_at = m + 1;  // walk ends after this shell
+    int stop_at = m + 1;  // the walk ends after this shell
     int s_end = 1;
-    unsigned long long cells_in = 1;
+    double cells_in = 1.0;
 
     for (int s = 2; s <= m; ++s) {
         const int st = __ldg(a.start + s);
         const int cnt = __ldg(a.count + s);
-        Kahan acc[22];
+        Kahan acc[13];
 #pragma unroll
-        for (int i = 0; i < 22; ++i) acc[i].zero();
+        for (int i = 0; i < 13; ++i) acc[i].zero();
         int nin = 0;
-        for (int c = lane; c < cnt; c += 32) {
+        for (int c = t; c < cnt; c += G) {
             const char4 o = __ldg(a.off + st + c);
             const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
             if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
+            const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
+                                  a.s2 * (iv3 - 1);
             float v[8];
-            CellLoader<PACKED>::load(a, iv1, iv2, iv3, v);
-            const float d[3] = {(float)o.x, (float)o.y, (float)o.z};
+            CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
+            const float d0 = (float)o.x, d1 = (float)o.y, d2 = (float)o.z;
             ++nin;
             acc[0].add(v[0]);
-#pragma unroll
-            for (int L = 0; L < 3; ++L) {
-                acc[1 + L].add(v[2 + L]);
-                acc[4 + L].add(v[5 + L]);
-                acc[7 + L].add(v[0] * d[L]);
-                acc[10 + L].add(v[1] * d[L]);
-#pragma unroll
-                for (int K = 0; K < 3; ++K) acc[13 + 3 * L + K].add(v[2 + L] * d[K]);
-            }
+            acc[1].add(v[0] * d0); acc[2].add(v[0] * d1); acc[3].add(v[0] * d2);
+            acc[4].add(v[1] * d0); acc[5].add(v[1] * d1); acc[6].add(v[1] * d2);
+            const float e0 = v[2], e1 = v[3], e2 = v[4];
+            acc[7].add(2.0f * (e0 * d0));
+            acc[8].add(2.0f * (e1 * d1));
+            acc[9].add(2.0f * (e2 * d2));
+            acc[10].add(e0 * d1 + e1 * d0);
+            acc[11].add(e0 * d2 + e2 * d0);
+            acc[12].add(e1 * d2 + e2 * d1);
         }
-        R[V_F * kRedPitch + lane] = acc[0].value();
-        R[V_N * kRedPitch + lane] = (double)nin;
+        // combine the lanes in FP64, lanes 0..G-1 in order (deterministic)
+        R[V_F * RP + t] = acc[0].value();
+        R[V_N * RP + t] = (double)nin;
 #pragma unroll
-        for (int L = 0; L < 3; ++L) {
-            R[(V_S + L) * kRedPitch + lane] = acc[1 + L].value();
-            R[(V_S2 + L) * kRedPitch + lane] = acc[4 + L].value();
-            R[(V_G + L) * kRedPitch + lane] = acc[7 + L].value();
-            R[(V_GF + L) * kRedPitch + lane] = acc[10 + L].value();
+        for (int i = 0; i < 12; ++i) R[(V_G + i) * RP + t] = acc[1 + i].value();
+        g.sync();
+        for (int v = t; v < V_ROWS; v += G) {
+            double sum = 0.0;
+            for (int u = 0; u < G; ++u) sum += R[v * RP + u];
+            R[v * RP + G] = sum;
         }
-#pragma unroll
-        for (int i = 0; i < 9; ++i) R[(V_SR + i) * kRedPitch + lane] = acc[13 + i].value();
-        const double mine = warp_column_sum(R, lane);
-
+        g.sync();
         // finalise shell s (ShellAnalysisGPU.jl:197-228)
-        const double Fs = __shfl_sync(0xffffffffu, mine, V_F);
-        const double ns = __shfl_sync(0xffffffffu, mine, V_N);
+        const double Fs = R[V_F * RP + G];
+        const double ns = R[V_N * RP + G];
         const double rs = rad[s];
         const double dF = ns > 0.0 ? Fs / ns : 0.0;
         const double r3p = radp * radp * radp, r3 = rs * rs * rs;
         const double Fbar_s = (r3p * Fbarp + 0.5 * (dFbarp + dF) * (r3 - r3p)) / r3;
         const double r5 = rs * rs * rs * rs * rs;
         csrb += 0.5 * (Fbarp + Fbar_s) * (r5 - rad5p);
-
-        // strain sums: lane 14 + 3L + K holds SR_LK; symmetrise with the partner KL
-        const int srl = lane - V_SR;
-        int partner = lane;
-        if (srl >= 0 && srl < 9) partner = V_SR + 3 * (srl % 3) + srl / 3;
-        const double norm = mine / rs;
-        const double pnorm = __shfl_sync(0xffffffffu, norm, partner);
         double* q = P + (size_t)s * kRec;
-        if (lane == V_F) q[P_FBAR] = Fbar_s;
-        if (lane >= V_G && lane < V_G + 6) q[P_G + (lane - V_G)] = norm;   // G then Gf
-        if (srl >= 0 && srl < 9) {
-            const int L = srl / 3, K = srl % 3;
-            int slot = -1;
-            if (L == K) slot = L;                      // 11, 22, 33
-            else if (L == 0 && K == 1) slot = 3;       // 12
-            else if (L == 0 && K == 2) slot = 4;       // 13
-            else if (L == 1 && K == 2) slot = 5;       // 23
-            if (slot >= 0) q[P_SR + slot] = norm + pnorm;
+        for (int i = t; i <= P_CSRB; i += G) {
+            double v;
+            if (i == P_FBAR) v = Fbar_s;
+            else if (i == P_CSRB) v = csrb;
+            else v = R[(V_G + i - P_G) * RP + G] / rs;   // G, Gf, SR rows follow in order
+            q[i] = v;
         }
-        if ((lane >= V_S && lane < V_S + 6) || lane == V_N) {
-            cum += mine;
-            const int slot = lane == V_N ? P_CN : P_CS + (lane - V_S);
-            q[slot] = cum;
-        }
-        if (lane == 31) q[P_CSRB] = csrb;
-        cells_in += (unsigned long long)ns;
-
+        g.sync();
+        cells_in += ns;
         Fbarp = Fbar_s; dFbarp = dF; radp = rs; rad5p = r5;
         s_end = s;
-
         // early exit: stop once every shell the post-processing reads is present --
         // Fbar up to the crossing m_c, gradients/strain of shells within r < rad[m0]+2
         // plus the first shell beyond it (zvir_half windows), and the mrf window.
-        if (m_c == 0 && s >= m0_init && Fbar_s < fcrit) {
+        if (m_c == 0 && s >= bd.m0_init && Fbar_s < fcrit) {
             m_c = s;
-            const int q2 = first_above(rad, s + 1, m, rad[s] + 2.0);
-            stop_at = max(q2, need_rf);
+            stop_at = max(first_above(rad, s + 1, m, rs + 2.0), bd.need_rf);
         }
         if (s >= stop_at) break;
     }
-    __syncwarp();
-    if (lane == 0 && a.stats) {
-        atomicAdd(a.stats, cells_in);
+    if (t == 0 && a.stats) {
+        atomicAdd(a.stats, (unsigned long long)cells_in);
         atomicAdd(a.stats + 1, (unsigned long long)s_end);
     }
 
     // ------------------------------------------------------ post-processing ----
-    // gradient at the filter scale (RadialShell.jl:466-482)
+    // gradient at the filter scale (RadialShell.jl:466-482); when mrf = 1 the window
+    // starts at the centre shell
     double gradpkrf[3];
     {
-        int lo, hi;
-        if (mrf > 1) {
-            lo = first_above(rad, 1, mrf, fmax(rad[mrf] - 2.0, 0.0));
-            if (lo > mrf) lo = mrf;
-        } else {
-            lo = 1;
-        }
-        hi = max(mrf, last_below(rad, mrf, m, rad[mrf] + 2.0));
-        Strain k = kernel_strain(P, rad, a.akk, mrf, lo, hi, a.wRnor, a.aRnor);
+        const Strain k = bd.mrf > 1 ? kernel_strain(a, P, bd.mrf, 1, bd.need_rf)
+                                    : kernel_strain_central(a, P, 1, bd.need_rf);
         gradpkrf[0] = k.g[0]; gradpkrf[1] = k.g[1]; gradpkrf[2] = k.g[2];
     }
 
     // crossing (RadialShell.jl:485-526)
-    int m0 = m0_init;
+    int m0 = bd.m0_init;
     if (P[(size_t)m0 * kRec + P_FBAR] >= fcrit) {
-        if (m_c != 0) m0 = m_c;   // else: no crossing, m0 stays, window up to m
+        if (m_c != 0) m0 = m_c;   // else: no crossing, m0 stays, windows reach m
     } else {
         // inward: first shell below m0_init (from the top) with Fbar >= fcrit
-        int found = 0;
-        for (int base = m0_init - 1; base >= 1 && !found; base -= 32) {
-            const int mp = base - lane;
+        bool found = false;
+        for (int base = bd.m0_init - 1; base >= 1 && !found; base -= G) {
+            const int mp = base - t;
             const bool ge = mp >= 1 && P[(size_t)mp * kRec + P_FBAR] >= fcrit;
-            const unsigned bal = __ballot_sync(0xffffffffu, ge);
+            const unsigned bal = g.ballot(ge);
             if (bal) {
-                const int l = __ffs(bal) - 1;
-                m0 = base - l + 1;
-                found = 1;
+                m0 = base - (__ffs(bal) - 1) + 1;
+                found = true;
             }
         }
-        if (!found) { write_no_collapse(a, p, lane); return; }
+        if (!found) { write_no_collapse(a, p, g); return; }
     }
 
-    // inward walk (RadialShell.jl:529-686): step t evaluates shell m0 - t; step 0 is
-    // m0 itself with zvir forced to -1 (RadialShell.jl:566-567).  Lanes evaluate 32
+    // inward walk (RadialShell.jl:529-686): step u evaluates shell m0 - u; step 0 is m0
+    // itself with zvir forced to -1 (RadialShell.jl:566-567).  The G lanes evaluate G
     // consecutive steps at once; the first step with zvir >= ZZon collapses.  Step
-    // results are staged in R (row = lane, row 32 = last step of the previous group).
+    // results are staged in R (row = lane, row G = last step of the previous round).
     int tstar = -1, lrow = 0, prow = 0;
-    for (int base = 0; base < m0; base += 32) {
-        const int t = base + lane;
-        double* row = R + lane * kStepW;
+    for (int base = 0; base < m0; base += G) {
+        const int u = base + t;
+        double* row = R + t * kStepW;
         bool hit = false;
-        if (t < m0) {
-            const Step st = eval_step(a, P, m0 - t, m, t == 0);
+        if (u < m0) {
+            const Step st = eval_step(a, P, m0 - u, m, u == 0);
 #pragma unroll
             for (int i = 0; i < 6; ++i) row[i] = st.k.E[i];
 #pragma unroll
@@ -667,19 +625,19 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
             row[13] = st.zvir;
             hit = st.zvir >= ZZon;
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-        __syncwarp();
+        const unsigned bal = g.ballot(hit);
+        g.sync();
         if (bal) {
             const int l = __ffs(bal) - 1;
             tstar = base + l;
             lrow = l;
-            prow = l > 0 ? l - 1 : 32;
+            prow = l > 0 ? l - 1 : G;
             break;
         }
-        if (lane < 14) R[32 * kStepW + lane] = R[31 * kStepW + lane];
-        __syncwarp();
+        for (int i = t; i < 14; i += G) R[G * kStepW + i] = R[(G - 1) * kStepW + i];
+        g.sync();
     }
-    if (tstar < 0 || (tstar == 0 && m0 == 1)) { write_no_collapse(a, p, lane); return; }
+    if (tstar < 0 || (tstar == 0 && m0 == 1)) { write_no_collapse(a, p, g); return; }
     if (tstar == 0) prow = lrow;
     const double* Lr = R + lrow * kStepW;   // collapse step ("last")
     const double* Pr = R + prow * kStepW;   // the step before it ("prev")
@@ -696,7 +654,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     } else {
         RTHL = rp;
     }
-    if (RTHL <= 0.0) { write_no_collapse(a, p, lane); return; }
+    if (RTHL <= 0.0) { write_no_collapse(a, p, g); return; }
 
     const double RTHL3 = RTHL * RTHL * RTHL, RTHL5 = RTHL3 * RTHL * RTHL;
     const double rad3p = rp * rp * rp, rad3 = rm * rm * rm, drad3 = rad3 - rad3p;
@@ -738,17 +696,45 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
 #pragma unroll
         for (int i = 0; i < 6; ++i) sfin[i] = Lr[i] * (Fbarx / Frhoh);
     }
-    // Sbar (RadialShell.jl:739-754) from the running sums at shell m0f - 1
-    const double* qp = P + (size_t)(m0f - 1) * kRec;
-    const double nS = qp[P_CN];
-    // Srb (RadialShell.jl:757-771)
-    double Srb = qp[P_CSRB];
+    // Srb (RadialShell.jl:757-771) from the running numerator at shell m0f - 1
+    double Srb = P[(size_t)(m0f - 1) * kRec + P_CSRB];
     const double r5p = m0f - 1 >= 2 ? rp * rp * rp * rp * rp : 0.0;
     if (zvir1 > 0.0 && dZ != 0.0) Srb += 0.5 * (Fb_p + Fbarx) * (RTHL5 - r5p);
     if (Fbarx * RTHL5 > 0.0) Srb /= (Fbarx * RTHL5);
+    g.sync();   // R is reused below
+
+    // Sbar, Sbar2 (RadialShell.jl:739-754): mean psi over the in-tile cells of shells
+    // 1..m0f-1, a contiguous prefix of the cell list
+    double Sb[3], Sb2[3];
+    {
+        const int ncell = __ldg(a.start + m0f);
+        Kahan ks[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) ks[i].zero();
+        int nloc = 0;
+        for (int c = t; c < ncell; c += G) {
+            const char4 o = __ldg(a.off + c);
+            const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
+            if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
+            const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
+                                  a.s2 * (iv3 - 1);
+            float v[8];
+            CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
+#pragma unroll
+            for (int i = 0; i < 6; ++i) ks[i].add(v[2 + i]);
+            ++nloc;
+        }
+        const double nS = g.sum((double)nloc);
+#pragma unroll
+        for (int L = 0; L < 3; ++L) {
+            const double s1 = g.sum(ks[L].value()), s2v = g.sum(ks[3 + L].value());
+            Sb[L] = nS > 0.0 ? s1 / nS : 0.0;
+            Sb2[L] = nS > 0.0 ? s2v / nS : 0.0;
+        }
+    }
 
     // cells with r <= RTHL: shells 1..s_in form a contiguous prefix of the cell list
-    const int s_in = last_le(rad, 1, nshells, RTHL);
+    const int s_in = last_le(rad, 1, a.nshells, RTHL);
     const int ncell_in = s_in >= 1 ? __ldg(a.start + s_in) + __ldg(a.count + s_in) : 0;
 
     // d2F
@@ -759,7 +745,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         if (a.conv == HT_CONV_GPU) {
             // all in-tile cells of shells with r <= RTHL, centre included
             // (ShellAnalysisGPU.jl:496-511)
-            for (int c = lane; c < ncell_in; c += 32) {
+            for (int c = t; c < ncell_in; c += G) {
                 const char4 o = __ldg(a.off + c);
                 const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
                 if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
@@ -771,8 +757,8 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         } else {
             // cells 2.. in shell order, stopping at the first out-of-tile cell
             // (RadialShell.jl:785-799)
-            for (int base = 1; base < ncell_in; base += 32) {
-                const int c = base + lane;
+            for (int base = 1; base < ncell_in; base += G) {
+                const int c = base + t;
                 bool oob = false;
                 int iv1 = 0, iv2 = 0, iv3 = 0;
                 if (c < ncell_in) {
@@ -780,9 +766,9 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
                     iv1 = ci + o.x; iv2 = cj + o.y; iv3 = ck + o.z;
                     oob = iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3;
                 }
-                const unsigned bal = __ballot_sync(0xffffffffu, oob);
-                const int lim = bal ? __ffs(bal) - 1 : 32;
-                if (c < ncell_in && lane < lim) {
+                const unsigned bal = g.ballot(oob);
+                const int lim = bal ? __ffs(bal) - 1 : G;
+                if (c < ncell_in && t < lim) {
                     const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
                                           a.s2 * (iv3 - 1);
                     ks.add(__ldg(a.lapd + idx));
@@ -791,14 +777,14 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
                 if (bal) break;
             }
         }
-        const double tot = warp_sum(ks.value());
-        const double nt = warp_sum((double)nloc);
+        const double tot = g.sum(ks.value());
+        const double nt = g.sum((double)nloc);
         if (nt > 0.0) d2F = tot / nt;
     }
 
     // mask: core cells within RTHL (ShellAnalysisGPU.jl:513-528, RadialShell.jl:773-782)
     if (a.mask) {
-        for (int c = lane; c < ncell_in; c += 32) {
+        for (int c = t; c < ncell_in; c += G) {
             const char4 o = __ldg(a.off + c);
             const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
             if (iv1 > a.nbuff && iv1 <= a.n1 - a.nbuff && iv2 > a.nbuff &&
@@ -810,13 +796,15 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         }
     }
 
-    // zvir_half (RadialShell.jl:801-859): lane jj-1 handles radius jj
+    // zvir_half (RadialShell.jl:801-859): radius jj is handled by lane (jj - 1) % G
     double zvir_half = -1.0;
     if (RTHL >= 3.0) {
-        double zl = -1.0;
+        double mx = -1.0;
         bool nan = false;
-        if (lane < 10) {
-            const double rcur = RTHL * pow(lane / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
+        for (int jj0 = 0; jj0 < 10; jj0 += G) {
+            const int jj = jj0 + t;   // 0-based radius index
+            if (jj >= 10) continue;
+            const double rcur = RTHL * pow(jj / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
             const int mm1 = m - 1;
             int mupp_rc = 1;
             if (mm1 >= 2) {
@@ -833,27 +821,26 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
                 const int f = first_above(rad, 1, mm1, rcur);
                 m0_rc = f <= mm1 ? f : mm1;
             }
-            const Strain k = kernel_strain(P, rad, a.akk, m0_rc, mlow_rc, mupp_rc, a.wRnor,
-                                           a.aRnor);
+            const Strain k = m0_rc > 1 ? kernel_strain(a, P, m0_rc, mlow_rc, mupp_rc)
+                                       : kernel_strain_central(a, P, mlow_rc, mupp_rc);
             const Shape sh = shape_of(k.E);
             const double Fc = P[(size_t)m0_rc * kRec + P_FBAR];
             const double poe = sh.e_v < 1e-5 ? 0.0 : sh.p_v / sh.e_v;
             double z = -1.0;
             if (Fc > 0.0) z = interp3(a, log10(Fc), sh.e_v, poe);
-            zl = z - 1.0;
-            nan = isnan(zl);
+            const double zl = z - 1.0;
+            if (isnan(zl)) nan = true;
+            else mx = fmax(mx, zl);
         }
         // Julia's max propagates NaN
-        const bool anynan = __any_sync(0xffffffffu, nan);
-        double mx = zl;
-#pragma unroll
-        for (int o = 16; o >= 1; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        zvir_half = anynan ? __longlong_as_double(0x7ff8000000000000ULL) : fmax(mx, -1.0);
+        const bool anynan = g.ballot(nan) != 0u;
+        for (int o = G >> 1; o >= 1; o >>= 1) mx = fmax(mx, __shfl_xor_sync(g.mask, mx, o, G));
+        zvir_half = anynan ? __longlong_as_double(0x7ff8000000000000ULL) : mx;
     }
 
     // outputs
     const ht_results& o = a.out;
-    if (lane == 0) {
+    if (t == 0) {
         o.RTHL[p] = (float)RTHL;
         o.Fbarx[p] = (float)Fbarx;
         o.e_v[p] = (float)fin.e_v;
@@ -862,55 +849,88 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         o.d2F[p] = (float)d2F;
         o.zvir_half[p] = (float)zvir_half;
     }
-    if (lane < 9) {
-        const int L = lane % 3, K = lane / 3;   // column-major (L, K)
+    for (int i = t; i < 9; i += G) {
+        const int L = i % 3, K = i / 3;   // column-major (L, K)
         int idx6;
         if (L == K) idx6 = L;
         else if (L + K == 1) idx6 = 3;
         else if (L + K == 2) idx6 = 4;
         else idx6 = 5;
-        o.strain[9 * p + lane] = (float)sfin[idx6];
+        o.strain[9 * p + i] = (float)sfin[idx6];
     }
-    if (lane < 3) {
-        const double cs = qp[P_CS + lane], cs2 = qp[P_CS2 + lane];
-        o.Sbar[3 * p + lane] = (float)(nS > 0.0 ? cs / nS : 0.0);
-        o.Sbar2[3 * p + lane] = (float)(nS > 0.0 ? cs2 / nS : 0.0);
-        o.gradpk[3 * p + lane] = (float)gpk[lane];
-        o.gradpkf[3 * p + lane] = (float)gpkf[lane];
-        o.gradpkrf[3 * p + lane] = (float)gradpkrf[lane];
-        o.eigs[3 * p + lane] = (float)fin.lam[lane];
+    if (t < 3) {
+        o.Sbar[3 * p + t] = (float)Sb[t];
+        o.Sbar2[3 * p + t] = (float)Sb2[t];
+        o.gradpk[3 * p + t] = (float)gpk[t];
+        o.gradpkf[3 * p + t] = (float)gpkf[t];
+        o.gradpkrf[3 * p + t] = (float)gradpkrf[t];
+        o.eigs[3 * p + t] = (float)fin.lam[t];
     }
+}
+
+// One work item: kPeaksPerItem consecutive peaks.  If all of them take G = 8, four
+// groups of 8 lanes run them side by side; otherwise they run one after the other, each
+// with its own G (lanes 8..31 idle for a G = 8 peak).  Group q of warp w owns scratch
+// slot 4 w + q.
+template <bool PACKED>
+__device__ void process_item(const WalkArgs& a, long long item, double* P0, double* W,
+                             int lane) {
+    const long long p0 = item * kPeaksPerItem;
+    const int np = (int)min((long long)kPeaksPerItem, a.npeaks - p0);
+    int gs[kPeaksPerItem];
+    bool all_small = np == kPeaksPerItem;
+    for (int k = 0; k < np; ++k) {
+        gs[k] = group_size(a, p0 + k);
+        all_small = all_small && gs[k] == kSmallG;
+    }
+    if (all_small) {
+        const int q = lane / kSmallG;
+        Group g{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
+        process_peak<PACKED>(a, p0 + q, P0 + q * a.scratch_stride,
+                             W + q * group_smem_doubles(kSmallG), g);
+    } else {
+        for (int k = 0; k < np; ++k) {
+            if (gs[k] == 32) {
+                Group g{32, lane, 0, 0xffffffffu};
+                process_peak<PACKED>(a, p0 + k, P0, W, g);
+            } else if (lane < kSmallG) {
+                Group g{kSmallG, lane, 0, (1u << kSmallG) - 1u};
+                process_peak<PACKED>(a, p0 + k, P0, W, g);
+            }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
 }
 
 template <bool PACKED>
 __global__ void __launch_bounds__(kThreads) walk_kernel(const WalkArgs a) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
-    double* R = smem + (threadIdx.x >> 5) * kWarpSmemDoubles;
+    double* W = smem + (threadIdx.x >> 5) * kWarpSmemDoubles;
     const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const long long nw = (long long)gridDim.x * kWarpsPerBlock;
-    double* P = a.scratch + gw * a.scratch_stride;
-    long long p;
+    double* P0 = a.scratch + gw * (32 / kSmallG) * a.scratch_stride;
+    const long long nitems = (a.npeaks + kPeaksPerItem - 1) / kPeaksPerItem;
+    long long item;
     if (a.dynamic) {
         int q = 0;
         if (lane == 0) q = atomicAdd(a.queue, 1);
-        p = __shfl_sync(0xffffffffu, q, 0);
+        item = __shfl_sync(0xffffffffu, q, 0);
     } else {
-        p = gw;
+        item = gw;
     }
-    while (p < a.npeaks) {
-        process_peak<PACKED>(a, p, P, R, lane);
-        __syncwarp();
+    while (item < nitems) {
+        process_item<PACKED>(a, item, P0, W, lane);
         if (a.dynamic) {
             int q = 0;
             if (lane == 0) q = atomicAdd(a.queue, 1);
-            p = __shfl_sync(0xffffffffu, q, 0);
+            item = __shfl_sync(0xffffffffu, q, 0);
         } else {
-            p += nw;
+            item += nw;
         }
     }
 }
-
 // Interleaved cell records: rec[2c] = (delta, delta[k,i,j], eta x, eta y),
 // rec[2c+1] = (eta z, eta2 x, eta2 y, eta2 z).  A 32x32 (i, k) tile of the transposed
 // read is staged through shared memory so both the reads and the record writes are
@@ -967,47 +987,10 @@ int ht_launch_pack(ht_ctx* ctx, cudaStream_t st) {
     return HT_OK;
 }
 
-int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rmax2rs,
-                   int32_t nbuff, int8_t* d_mask, int32_t conv, int32_t mode,
-                   const ht_results* out, cudaStream_t st) {
-    const bool packed = mode == HT_MODE_BATCHED;
-    const size_t smem = (size_t)kWarpsPerBlock * kWarpSmemDoubles * sizeof(double);
-    int bpsm = 0;
-    cudaError_t e;
-    if (packed) {
-        e = cudaFuncSetAttribute(walk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<true>, kThreads,
-                                                              smem);
-    } else {
-        e = cudaFuncSetAttribute(walk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<false>, kThreads,
-                                                              smem);
-    }
-    if (e != cudaSuccess) return ht_cuda_fail(e, "occupancy query");
-    if (bpsm < 1) bpsm = 1;
-    long long blocks = (long long)ctx->num_sms * bpsm;
-    const long long warps_needed = (b->npeaks + 0);
-    if (!packed) {
-        // static schedule: no more warps than peaks
-        long long bl = (warps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        if (bl < blocks) blocks = bl;
-    } else {
-        long long bl = (warps_needed + kWarpsPerBlock - 1) / kWarpsPerBlock;
-        if (bl < blocks) blocks = bl;
-    }
-    if (blocks < 1) blocks = 1;
-    const long long nwarps = blocks * kWarpsPerBlock;
-    const long long stride = (long long)(ctx->nshells + 2) * kRec;
-    const size_t need = (size_t)nwarps * stride * sizeof(double);
-    int rc = ht_grow((void**)&ctx->d_scratch, &ctx->scratch_bytes, need, "shell-walk scratch");
-    if (rc != HT_OK) return rc;
-
-    WalkArgs a;
-    const ht_fields& f = ctx->fields;
+// Fill the kernel arguments common to both entry points.
+static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const ht_peak_batch* b,
+                      double alatt, double rmax2rs, int32_t nbuff, int8_t* d_mask, int32_t conv,
+                      const ht_results* out) {
     a.rec = ctx->d_rec;
     a.delta = f.delta; a.ex = f.etax; a.ey = f.etay; a.ez = f.etaz;
     a.e2x = f.eta2x; a.e2y = f.eta2y; a.e2z = f.eta2z; a.lapd = f.lapd;
@@ -1015,6 +998,7 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     a.s2 = (long long)f.n1 * f.n2;
     a.off = ctx->d_off; a.start = ctx->d_start; a.count = ctx->d_count; a.r2 = ctx->d_r2;
     a.rad = ctx->d_rad; a.nshells = ctx->nshells;
+    a.wrow = ctx->d_wrow; a.wm1 = ctx->d_wm1; a.wwt = ctx->d_wwt;
     a.ct = ctx->d_ct; a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz;
     a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
     a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
@@ -1025,20 +1009,60 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     a.aRnor = 3.0 / alatt;                   // RadialShell.jl:296-300 with hlatt = 1
     a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
     a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
+    a.small_max_shells = ctx->small_max_shells;
+    a.queue = nullptr; a.dynamic = 0; a.stats = nullptr;
+}
+
+static size_t walk_smem_bytes() {
+    return (size_t)kWarpsPerBlock * kWarpSmemDoubles * sizeof(double);
+}
+
+template <bool PACKED>
+static int walk_blocks_per_sm(int* bpsm) {
+    const size_t smem = walk_smem_bytes();
+    cudaError_t e = cudaFuncSetAttribute(walk_kernel<PACKED>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(bpsm, walk_kernel<PACKED>, kThreads,
+                                                          smem);
+    if (e != cudaSuccess) return ht_cuda_fail(e, "walk_kernel occupancy query");
+    if (*bpsm < 1) *bpsm = 1;
+    return HT_OK;
+}
+
+int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rmax2rs,
+                   int32_t nbuff, int8_t* d_mask, int32_t conv, int32_t mode,
+                   const ht_results* out, cudaStream_t st) {
+    const bool packed = mode == HT_MODE_BATCHED;
+    int bpsm = 0;
+    int rc = packed ? walk_blocks_per_sm<true>(&bpsm) : walk_blocks_per_sm<false>(&bpsm);
+    if (rc != HT_OK) return rc;
+    long long blocks = (long long)ctx->num_sms * bpsm;
+    const long long items = (b->npeaks + kPeaksPerItem - 1) / kPeaksPerItem;
+    const long long need = (items + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (blocks > need) blocks = need;
+    if (blocks < 1) blocks = 1;
+    const long long stride = (long long)(ctx->nshells + 2) * kRec;
+    const size_t slots = (size_t)blocks * kWarpsPerBlock * (32 / kSmallG);
+    rc = ht_grow((void**)&ctx->d_scratch, &ctx->scratch_bytes, slots * stride * sizeof(double),
+                 "shell-walk scratch");
+    if (rc != HT_OK) return rc;
+
+    WalkArgs a;
+    fill_args(a, ctx, ctx->fields, b, alatt, rmax2rs, nbuff, d_mask, conv, out);
     a.scratch = ctx->d_scratch; a.scratch_stride = stride;
     a.queue = ctx->d_queue; a.dynamic = packed ? 1 : 0;
     a.stats = ctx->d_stats;
-
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st), "queue reset");
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_stats, 0, 2 * sizeof(unsigned long long), st),
                 "stats reset");
+    const size_t smem = walk_smem_bytes();
     if (packed) walk_kernel<true><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     else walk_kernel<false><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch");
     ctx->last_kernels = 1;
     return HT_OK;
 }
-
 // ------------------------------------------------- allocation-free entry point ----
 //
 // ht_shell_analyse_static: the shell collapse for callers that must not allocate device
@@ -1103,9 +1127,10 @@ extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
     if (nbuff < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: nbuff < 0");
     if (ctx->nshells < 3)
         return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: hunt radius too small");
-    // one 8-warp block must fit the static scratch
+    // one block (8 warps x 4 group slots) must fit the static scratch
     const long long stride = (long long)(ctx->nshells + 2) * kRec;
-    const size_t per_block = (size_t)kWarpsPerBlock * stride * sizeof(double);
+    const size_t per_block =
+        (size_t)kWarpsPerBlock * (32 / kSmallG) * stride * sizeof(double);
     if (per_block > kStaticScratchBytes)
         return ht_fail(HT_ERR_CAPACITY,
                        "ht_shell_analyse_static: the hunt radius needs " +
@@ -1117,41 +1142,23 @@ extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
     void* scratch = nullptr;
     int rc = static_scratch_address(ctx->device, &scratch);
     if (rc != HT_OK) return rc;
-
-    const size_t smem = (size_t)kWarpsPerBlock * kWarpSmemDoubles * sizeof(double);
-    cudaError_t e = cudaFuncSetAttribute(walk_kernel<false>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return ht_cuda_fail(e, "cudaFuncSetAttribute");
     int bpsm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, walk_kernel<false>, kThreads, smem);
-    if (e != cudaSuccess) return ht_cuda_fail(e, "occupancy query");
-    long long blocks = (long long)ctx->num_sms * (bpsm > 0 ? bpsm : 1);
+    rc = walk_blocks_per_sm<false>(&bpsm);
+    if (rc != HT_OK) return rc;
+    long long blocks = (long long)ctx->num_sms * bpsm;
     const long long fit = (long long)(kStaticScratchBytes / per_block);
-    const long long need = (b->npeaks + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    const long long items = (b->npeaks + kPeaksPerItem - 1) / kPeaksPerItem;
+    const long long need = (items + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (blocks > fit) blocks = fit;
     if (blocks > need) blocks = need;
 
     WalkArgs a;
+    fill_args(a, ctx, *f, b, alatt, rmax2rs, nbuff, d_mask, conv, out);
     a.rec = nullptr;
-    a.delta = f->delta; a.ex = f->etax; a.ey = f->etay; a.ez = f->etaz;
-    a.e2x = f->eta2x; a.e2y = f->eta2y; a.e2z = f->eta2z; a.lapd = f->lapd;
-    a.n1 = f->n1; a.n2 = f->n2; a.n3 = f->n3;
-    a.s2 = (long long)f->n1 * f->n2;
-    a.off = ctx->d_off; a.start = ctx->d_start; a.count = ctx->d_count; a.r2 = ctx->d_r2;
-    a.rad = ctx->d_rad; a.nshells = ctx->nshells;
-    a.ct = ctx->d_ct; a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz;
-    a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
-    a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
-    a.pi = b->pi; a.pj = b->pj; a.pk = b->pk; a.Rf = b->Rf; a.ir2min = b->ir2min;
-    a.ZZon = b->ZZon; a.fcrit = b->fcrit; a.npeaks = b->npeaks;
-    a.alatt = alatt;
-    const double pi = 3.14159265358979323846;
-    a.aRnor = 3.0 / alatt;
-    a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
-    a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
     a.scratch = (double*)scratch; a.scratch_stride = stride;
-    a.queue = nullptr; a.dynamic = 0;   // static peak-to-warp schedule: no counter to clear
+    a.queue = nullptr; a.dynamic = 0;   // static item-to-warp schedule: no counter to clear
     a.stats = nullptr;
+    const size_t smem = walk_smem_bytes();
     walk_kernel<false><<<(unsigned)blocks, kThreads, smem, (cudaStream_t)stream>>>(a);
     HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch (static scratch)");
     ctx->last_kernels = 1;

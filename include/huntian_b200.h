@@ -197,9 +197,9 @@ HT_API int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* batch, double alat
  *   stream capture begins.
  * - All calls share the one array: calls whose kernels overlap on the GPU (e.g. on two
  *   streams, or from two threads) race on it and give wrong results.  Serialize them.
- * - Limit: the hunt radius must leave one 8-warp block's scratch,
- *   8 * (nshells + 2) * 192 bytes, within 32 MiB (always true for nhunt <= 127);
- *   otherwise HT_ERR_CAPACITY.  Larger hunt radii run fewer concurrent warps. */
+ * - Limit: one 8-warp block's scratch, 8 warps * 4 peak slots * (nshells + 2) * 128 bytes,
+ *   must fit within 32 MiB, i.e. nshells <= 8190 (nhunt up to about 98); larger hunt
+ *   radii return HT_ERR_CAPACITY.  Larger hunt radii run fewer concurrent warps. */
 HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
                                    const ht_peak_batch* batch, double alatt, double rmax2rs,
                                    int32_t nbuff, int8_t* d_mask, int32_t conv,
