@@ -28,6 +28,7 @@ import tempfile
 import time
 
 import numpy as np
+import torch
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
@@ -152,7 +153,6 @@ def make_inputs(ht, wl, seed, device):
 
 class Workload:
     def __init__(self, ht, name, seed, device, mode):
-        import torch
         self.ht, self.name, self.wl, self.mode = ht, name, WORKLOADS[name], mode
         wl = self.wl
         self.device = device
@@ -177,7 +177,10 @@ class Workload:
 
     def smooth(self, Rf):
         from huntian_b200 import synth
-        return synth.smooth_padded(self.dk, self.n, self.wl["L"], Rf, 1, self.nbuff)
+        if getattr(self, "_work", None) is None or self._work.shape != self.dk.shape:
+            self._work = torch.empty_like(self.dk)
+        return synth.smooth_padded(self.finder, self.dk, self.n, self.wl["L"], Rf, 1,
+                                   self.nbuff, work=self._work)
 
     def step(self, ev=None):
         """One tile: peak scan over all filters, then pack + shell collapse."""

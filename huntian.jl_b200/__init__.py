@@ -7,11 +7,11 @@ host-side mirror of the reference's GPU entry points; see host.py.
 from ._lib import (HT_CONV_CPU, HT_CONV_GPU, HT_MODE_BATCHED, HT_MODE_PLAIN, HTError,
                    LIB_PATH, RESULT_NAMES, RESULT_WIDTH, SYMBOLS)
 from .host import (HaloFinder, PeakCandidate, analyse_peaks_gpu_cuda_multirf, ir2min_of,
-                   nhunt_of, peak_find_tile_gpu, smooth_field, smooth_window)
+                   nhunt_of, peak_find_tile_gpu)
 from .tables import log_filterbank, read_filterbank, read_homeltab, write_homeltab
 
 __all__ = ["HaloFinder", "PeakCandidate", "peak_find_tile_gpu",
-           "analyse_peaks_gpu_cuda_multirf", "smooth_field", "smooth_window", "ir2min_of",
+           "analyse_peaks_gpu_cuda_multirf", "ir2min_of",
            "nhunt_of", "read_homeltab", "write_homeltab", "read_filterbank",
            "log_filterbank", "HTError", "LIB_PATH", "SYMBOLS", "RESULT_NAMES",
            "RESULT_WIDTH", "HT_CONV_GPU", "HT_CONV_CPU", "HT_MODE_PLAIN", "HT_MODE_BATCHED"]

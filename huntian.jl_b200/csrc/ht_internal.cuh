@@ -54,6 +54,8 @@ struct ht_ctx {
     size_t pf_ws_bytes = 0;
     double* d_scratch = nullptr;   // shell-walk per-warp profiles
     size_t scratch_bytes = 0;
+    void* d_win = nullptr;         // smoothing-window table
+    size_t win_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked
 

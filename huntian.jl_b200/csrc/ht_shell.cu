@@ -252,44 +252,28 @@ __device__ __noinline__ Strain kernel_strain_central(const WalkArgs& a,
     return s;
 }
 
-// Ascending eigenvalues of a symmetric 3x3 matrix by cyclic Jacobi rotations in FP64
-// (Golub & Van Loan, Alg. 8.4.3), replacing LAPACK eigvals(Symmetric)
-// (RadialShell.jl:215-220).  E = (11, 22, 33, 12, 13, 23).
+// Ascending eigenvalues of a symmetric 3x3 matrix in FP64 by the trigonometric solution
+// of the characteristic cubic (O. K. Smith, Comm. ACM 4(4):168, 1961), replacing LAPACK
+// eigvals(Symmetric) (RadialShell.jl:215-220).  E = (11, 22, 33, 12, 13, 23).
 __device__ __noinline__ void eig3(const double* E, double* lam) {
-    double a[3][3];
-    a[0][0] = E[0]; a[1][1] = E[1]; a[2][2] = E[2];
-    a[0][1] = a[1][0] = E[3];
-    a[0][2] = a[2][0] = E[4];
-    a[1][2] = a[2][1] = E[5];
-    for (int sweep = 0; sweep < 64; ++sweep) {
-        double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
-        double dia = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
-        if (off == 0.0 || off <= 1e-40 * dia) break;
-#pragma unroll
-        for (int pq = 0; pq < 3; ++pq) {
-            const int p = pq == 2 ? 1 : 0;
-            const int q = pq == 0 ? 1 : 2;
-            double apq = a[p][q];
-            if (apq == 0.0) continue;
-            double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
-            double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
-            double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                double akp = a[k][p], akq = a[k][q];
-                a[k][p] = c * akp - sn * akq;
-                a[k][q] = sn * akp + c * akq;
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                double apk = a[p][k], aqk = a[q][k];
-                a[p][k] = c * apk - sn * aqk;
-                a[q][k] = sn * apk + c * aqk;
-            }
-            a[p][q] = a[q][p] = 0.0;
-        }
-    }
-    double e0 = a[0][0], e1 = a[1][1], e2 = a[2][2], t;
+    const double a11 = E[0], a22 = E[1], a33 = E[2], a12 = E[3], a13 = E[4], a23 = E[5];
+    const double q = (a11 + a22 + a33) / 3.0;
+    const double b11 = a11 - q, b22 = a22 - q, b33 = a33 - q;
+    const double off = a12 * a12 + a13 * a13 + a23 * a23;
+    const double p2 = (b11 * b11 + b22 * b22 + b33 * b33 + 2.0 * off) / 6.0;
+    if (!(p2 > 0.0)) { lam[0] = lam[1] = lam[2] = q; return; }
+    const double pp = sqrt(p2);
+    const double ip = 1.0 / pp;
+    const double c11 = b11 * ip, c22 = b22 * ip, c33 = b33 * ip;
+    const double c12 = a12 * ip, c13 = a13 * ip, c23 = a23 * ip;
+    double r = 0.5 * (c11 * (c22 * c33 - c23 * c23) - c12 * (c12 * c33 - c23 * c13) +
+                      c13 * (c12 * c23 - c22 * c13));
+    r = fmin(1.0, fmax(-1.0, r));
+    const double phi = acos(r) / 3.0;
+    double e2 = q + 2.0 * pp * cos(phi);
+    double e0 = q + 2.0 * pp * cos(phi + 2.0943951023931957);
+    double e1 = 3.0 * q - e0 - e2;
+    double t;
     if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
     if (e1 > e2) { t = e1; e1 = e2; e2 = t; }
     if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
@@ -903,8 +887,9 @@ __device__ void process_item(const WalkArgs& a, long long item, double* P0, doub
     __syncwarp();
 }
 
+// 3 blocks per SM: 80 registers; the few spills cost less than the lost occupancy.
 template <bool PACKED>
-__global__ void __launch_bounds__(kThreads) walk_kernel(const WalkArgs a) {
+__global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     double* W = smem + (threadIdx.x >> 5) * kWarpSmemDoubles;

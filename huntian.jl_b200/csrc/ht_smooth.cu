@@ -1,0 +1,93 @@
+// k-space smoothing window applied to the rfft of delta before the per-filter inverse
+// FFT (Filters.smooth_field, Filters.jl:72-99; GPU _smooth_window_kernel!,
+// ext/CUDAExt.jl:2831-2871).  The window depends on |k| only, and on the rfft grid
+// k^2 = dk^2 (ix^2 + iy^2 + iz^2) takes at most 3 (n/2)^2 + 1 values, so the FP64 window
+// is evaluated once per distinct integer ix^2 + iy^2 + iz^2 into a table (first kernel)
+// and the modes are multiplied by Float32(W) from it (second kernel, bandwidth-bound:
+// 8 B read + 8 B written per mode).  k = 0 is left unchanged, as in the reference.
+#include <math.h>
+
+#include "ht_internal.cuh"
+
+namespace {
+
+// wsmooth: 0 Gaussian in the Fortran convention exp(-(kR/2)^2 / 2), 3 the same times k^2,
+// anything else the top-hat 3 (sin x - x cos x) / x^3 (ext/CUDAExt.jl:2853-2866).
+__global__ void window_table_kernel(float* __restrict__ tab, int nvals, double dk, double Rf,
+                                    int wsmooth) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nvals) return;
+    double w = 1.0;
+    if (q > 0) {
+        const double k2 = (double)q * dk * dk;
+        const double k = sqrt(k2);
+        const double kR = k * Rf;
+        if (wsmooth == 0) {
+            w = exp(-kR * kR * 0.125);
+        } else if (wsmooth == 3) {
+            w = exp(-kR * kR * 0.125) * k2;
+        } else {
+            double s, c;
+            sincos(kR, &s, &c);
+            w = 3.0 * (s - kR * c) / (kR * kR * kR);
+        }
+    }
+    tab[q] = (float)w;
+}
+
+__global__ void __launch_bounds__(256) window_apply_kernel(const float2* __restrict__ in,
+                                                           float2* __restrict__ out, int n,
+                                                           const float* __restrict__ tab) {
+    const int nk = n / 2 + 1;
+    const long long total = (long long)nk * n * n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long li = (long long)blockIdx.x * blockDim.x + threadIdx.x; li < total;
+         li += stride) {
+        const int ix = (int)(li % nk);
+        const long long rem = li / nk;
+        const int iy = (int)(rem % n);
+        const int iz = (int)(rem / n);
+        const int sy = iy <= n / 2 ? iy : iy - n;
+        const int sz = iz <= n / 2 ? iz : iz - n;
+        const int q = ix * ix + sy * sy + sz * sz;
+        float2 v = in[li];
+        if (q > 0) {
+            const float w = __ldg(tab + q);
+            v.x *= w;
+            v.y *= w;
+        }
+        out[li] = v;
+    }
+}
+
+}  // namespace
+
+extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int n,
+                                       double boxsize, double Rf, int wsmooth, void* stream) {
+    if (!ctx || !d_delta_k || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: NULL argument");
+    if (n < 2 || n > 65536) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: n out of range");
+    if (!(boxsize > 0.0) || !(Rf >= 0.0))
+        return ht_fail(HT_ERR_INVALID, "ht_smooth_window: boxsize must be > 0 and Rf >= 0");
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_smooth_window");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const int h = n / 2;
+    const int nvals = 3 * h * h + 1;
+    int rc = ht_grow(&ctx->d_win, &ctx->win_bytes, (size_t)nvals * sizeof(float),
+                     "window table");
+    if (rc != HT_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const double dk = 2.0 * 3.14159265358979323846 / boxsize;
+    window_table_kernel<<<(nvals + 255) / 256, 256, 0, st>>>((float*)ctx->d_win, nvals, dk, Rf,
+                                                             wsmooth);
+    HT_CUDA_TRY(cudaGetLastError(), "window_table_kernel launch");
+    const long long total = (long long)(h + 1) * n * n;
+    long long blocks = (total + 255) / 256;
+    const long long cap = (long long)ctx->num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    window_apply_kernel<<<(unsigned)blocks, 256, 0, st>>>((const float2*)d_delta_k,
+                                                          (float2*)d_out, n,
+                                                          (const float*)ctx->d_win);
+    HT_CUDA_TRY(cudaGetLastError(), "window_apply_kernel launch");
+    ctx->last_kernels = 2;
+    return HT_OK;
+}

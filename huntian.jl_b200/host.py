@@ -103,6 +103,27 @@ class HaloFinder:
         check(_lib.load().ht_fsc_of_z(self._h, float(z), C.byref(v)))
         return v.value
 
+    # ------------------------------------------------------------ smoothing ----
+    def smooth_window(self, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
+                      wsmooth: int, out: Optional[torch.Tensor] = None, stream=None):
+        """delta_k (complex64 rfft of an n^3 field, shape (n, n, n//2+1)) times the
+        Float32 window of Filters.smooth_field (Filters.jl:72-99); out may alias delta_k."""
+        if delta_k.dtype != torch.complex64 or tuple(delta_k.shape) != (n, n, n // 2 + 1):
+            raise ValueError(f"delta_k must be complex64 of shape {(n, n, n // 2 + 1)}, got "
+                             f"{delta_k.dtype} {tuple(delta_k.shape)}")
+        delta_k = delta_k.contiguous()
+        out = torch.empty_like(delta_k) if out is None else out
+        check(_lib.load().ht_smooth_window(self._h, delta_k.data_ptr(), out.data_ptr(), int(n),
+                                           float(boxsize), float(Rf), int(wsmooth),
+                                           _stream_handle(stream)))
+        return out
+
+    def smooth_field(self, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
+                     wsmooth: int, work: Optional[torch.Tensor] = None) -> torch.Tensor:
+        """Filters.smooth_field: window (library kernel) then the cuFFT inverse rfft."""
+        w = self.smooth_window(delta_k, n, boxsize, Rf, wsmooth, out=work)
+        return torch.fft.irfftn(w, s=(n, n, n), dim=(0, 1, 2)).contiguous()
+
     # ---------------------------------------------------------------- peaks ----
     def peakfind_filter(self, delta_s: torch.Tensor, mask: torch.Tensor, nbuff: int,
                         fcrit: float, filter_idx: int, max_peaks: int, out: dict,
@@ -193,35 +214,6 @@ class HaloFinder:
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
 
 
-# ------------------------------------------------------------ smoothing (stays) ----
-
-def smooth_window(n: int, boxsize: float, Rf: float, wsmooth: int, device) -> torch.Tensor:
-    """k-space window of Filters.smooth_field (Filters.jl:72-99) on the rfft grid
-    (n, n, n//2+1), Float32, W(k=0) = 1.  0 = Gaussian (R/2 convention), 1 = top-hat,
-    3 = k^2 Gaussian."""
-    dk = 2.0 * math.pi / boxsize
-    kx = torch.arange(n // 2 + 1, device=device, dtype=torch.float64) * dk
-    kf = torch.fft.fftfreq(n, d=1.0 / n, device=device).to(torch.float64) * dk
-    k2 = kf.view(-1, 1, 1) ** 2 + kf.view(1, -1, 1) ** 2 + kx.view(1, 1, -1) ** 2
-    k = torch.sqrt(k2)
-    x = k * Rf
-    if wsmooth == 0:
-        w = torch.exp(-(x * 0.5) ** 2 / 2)
-    elif wsmooth == 3:
-        w = torch.exp(-(x * 0.5) ** 2 / 2) * k2
-    else:
-        w = 3.0 * (torch.sin(x) - x * torch.cos(x)) / (x * x * x)
-    w = torch.where(x == 0, torch.ones_like(w), w)
-    return w.to(torch.float32)
-
-
-def smooth_field(delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
-                 wsmooth: int) -> torch.Tensor:
-    """irfft(delta_k * W) with torch/cuFFT (the FFT filtering outside the hot path)."""
-    w = smooth_window(n, boxsize, Rf, wsmooth, delta_k.device)
-    return torch.fft.irfftn(delta_k * w, s=(n, n, n), dim=(0, 1, 2)).contiguous()
-
-
 # ----------------------------------------------------------- reference mirrors ----
 
 @dataclass
@@ -258,11 +250,12 @@ def peak_find_tile_gpu(delta_tile, filters: Sequence, fcrits: Sequence[float], t
     boxsize = n * float(alatt)   # periodic tile: boxsize_local = n * alatt
     has_lapd = ioutshear >= 1
     delta_k = torch.fft.rfftn(delta, dim=(0, 1, 2))
+    work = torch.empty_like(delta_k)
     out = HaloFinder.alloc_peaks(max_peaks, device, has_lapd)
     for fi, (flt, fc) in enumerate(zip(filters, fcrits), start=1):
         Rf = float(flt[2])
-        ds = smooth_field(delta_k, n, boxsize, Rf, wsmooth)
-        ls = smooth_field(delta_k, n, boxsize, Rf, 3) if has_lapd else None
+        ds = finder.smooth_field(delta_k, n, boxsize, Rf, wsmooth, work=work)
+        ls = finder.smooth_field(delta_k, n, boxsize, Rf, 3, work=work) if has_lapd else None
         finder.peakfind_filter(ds, mask, nbuff, float(np.float32(fc)), fi, max_peaks, out,
                                lapd_s=ls)
         del ds, ls

@@ -145,7 +145,7 @@ def gaussian_box(n: int, boxsize: float, seed: int, cosmo: Cosmology, device):
         amp = torch.where(k == 0, torch.zeros_like(amp), amp)
         dk_[z0:z1] *= amp
         del k, lnk, idx, t, lnp, amp
-    return dk_
+    return dk_.contiguous()
 
 
 def _irfft(a: torch.Tensor, n: int) -> torch.Tensor:
@@ -189,14 +189,14 @@ def laplacian(delta_k: torch.Tensor, n: int, boxsize: float) -> torch.Tensor:
 
 def wrap_pad(f: torch.Tensor, nbuff: int) -> torch.Tensor:
     """Periodic box (n^3) -> tile (n + 2 nbuff)^3 with periodic wrap in every direction."""
-    n = f.shape[0]
-    idx = torch.remainder(torch.arange(-nbuff, n + nbuff, device=f.device), n)
-    return f.index_select(0, idx).index_select(1, idx).index_select(2, idx).contiguous()
+    if nbuff == 0:
+        return f.contiguous()
+    import torch.nn.functional as F
+    return F.pad(f[None, None], (nbuff,) * 6, mode="circular")[0, 0].contiguous()
 
 
-def smooth_padded(delta_k: torch.Tensor, n: int, boxsize: float, Rf: float, wsmooth: int,
-                  nbuff: int) -> torch.Tensor:
-    """Filters.smooth_field on the periodic box (cuFFT), padded to the tile."""
-    from .host import smooth_window
-    w = smooth_window(n, boxsize, Rf, wsmooth, delta_k.device)
-    return wrap_pad(_irfft(delta_k * w, n), nbuff)
+def smooth_padded(finder, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
+                  wsmooth: int, nbuff: int, work=None) -> torch.Tensor:
+    """Filters.smooth_field on the periodic box (library window + cuFFT), padded to the
+    tile."""
+    return wrap_pad(finder.smooth_field(delta_k, n, boxsize, Rf, wsmooth, work=work), nbuff)

@@ -24,6 +24,7 @@
  *                          ext/CUDAExt.jl:1213-1912
  *   ht_ctx_create       -> per-call uploads of ShellTablesGPU (ext/CUDAExt.jl:16-41), the
  *                          collapse table and the SPH table (ext/CUDAExt.jl:45-52)
+ *   ht_smooth_window    -> ext/CUDAExt.jl:2831-2871 `_smooth_window_kernel!`
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  */
@@ -113,6 +114,15 @@ typedef struct {
 HT_API int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_s,
                        int8_t* d_mask, int n, int nbuff, float fcrit, int32_t filter_idx,
                        int64_t max_peaks, const ht_peaks* out, void* stream);
+
+/* Smoothing window for the per-filter peak scan: d_out = d_delta_k * Float32(W(|k| Rf))
+ * on the rfft grid of an n^3 periodic field of side `boxsize` (complex64, layout
+ * (n/2+1, n, n) column-major, i.e. what cuFFT's R2C of the column-major field gives),
+ * k = 0 unchanged; wsmooth 0 = Gaussian exp(-(kR/2)^2/2), 3 = that times k^2, otherwise
+ * the top-hat 3(sin x - x cos x)/x^3, W evaluated in FP64.  In place is allowed.
+ * Replaces ext/CUDAExt.jl:2831-2871 `_smooth_window_kernel!` (Filters.jl:72-99). */
+HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int n,
+                            double boxsize, double Rf, int wsmooth, void* stream);
 
 /* ------------------------------------------------------------ shell collapse ---- */
 

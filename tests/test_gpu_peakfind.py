@@ -107,3 +107,32 @@ def test_lapd_sampled_at_peaks(ht, oracle, finder):
     g = _both(ht, oracle, finder, fields, 2, [0.5], lapd=lap)
     idx = (g["k"] - 1, g["j"] - 1, g["i"] - 1)
     assert np.array_equal(g["lapd"], lap[0][idx])
+
+
+@pytest.mark.parametrize("wsmooth", [0, 1, 3])
+def test_smoothing_window(ht, finder, wsmooth):
+    """ht_smooth_window vs the FP64 window of Filters.smooth_field (Filters.jl:72-99)."""
+    import torch
+    n, box, Rf = 24, 60.0, 7.5
+    rng = np.random.default_rng(wsmooth)
+    a = rng.standard_normal((n, n, n)).astype(np.float32)
+    ak = np.fft.rfftn(a).astype(np.complex64)
+    dk = 2 * np.pi / box
+    kz = np.fft.fftfreq(n, 1.0 / n) * dk
+    kx = np.arange(n // 2 + 1) * dk
+    k2 = kz[:, None, None] ** 2 + kz[None, :, None] ** 2 + kx[None, None, :] ** 2
+    k = np.sqrt(k2)
+    x = k * Rf
+    with np.errstate(invalid="ignore", divide="ignore"):
+        if wsmooth == 0:
+            w = np.exp(-x * x / 8)
+        elif wsmooth == 3:
+            w = np.exp(-x * x / 8) * k2
+        else:
+            w = 3 * (np.sin(x) - x * np.cos(x)) / x ** 3
+    w = np.where(k2 == 0, 1.0, w).astype(np.float32)
+    ref = ak * w
+    got = finder.smooth_window(torch.as_tensor(ak, device="cuda"), n, box, Rf, wsmooth)
+    got = got.cpu().numpy()
+    assert np.allclose(got, ref, rtol=1e-6, atol=1e-6 * np.abs(ref).max())
+    assert got[0, 0, 0] == ak[0, 0, 0]
