@@ -167,7 +167,7 @@ class Workload:
         self.fcrit = float(np.float32(self.finder.fsc_of_z(0.0)))
         self.dk, self.tile = make_inputs(ht, wl, seed, device)
         self.mask = torch.zeros((self.nt,) * 3, dtype=torch.int8, device=device)
-        self.max_peaks = 16_000_000 if self.n >= 1024 else 4_000_000
+        self.max_peaks = 48_000_000 if self.n >= 1024 else 6_000_000
         self.peaks = ht.HaloFinder.alloc_peaks(self.max_peaks, device, False)
         self.Rf_f = torch.tensor([f[2] for f in self.filters], dtype=torch.float64, device=device)
         self.ir2_f = torch.tensor([ht.ir2min_of(f[2], self.alatt) for f in self.filters],
@@ -176,11 +176,10 @@ class Workload:
         self.npeaks = 0
 
     def smooth(self, Rf):
-        from huntian_b200 import synth
-        if getattr(self, "_work", None) is None or self._work.shape != self.dk.shape:
-            self._work = torch.empty_like(self.dk)
-        return synth.smooth_padded(self.finder, self.dk, self.n, self.wl["L"], Rf, 1,
-                                   self.nbuff, work=self._work)
+        if getattr(self, "_ds", None) is None:
+            self._ds = torch.empty((self.nt,) * 3, dtype=torch.float32, device=self.device)
+        return self.finder.smooth_tile(self.dk, self.n, self.nbuff, self.wl["L"], Rf, 1,
+                                       out=self._ds)
 
     def step(self, ev=None):
         """One tile: peak scan over all filters, then pack + shell collapse."""

@@ -27,7 +27,8 @@ HT_MODE_BATCHED = 1
 
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
-           "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_smooth_window", "ht_peakfind_filter",
+           "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_smooth_window", "ht_smooth_filter",
+           "ht_peakfind_filter",
            "ht_fields_pack",
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats")
 
@@ -97,6 +98,8 @@ def load() -> C.CDLL:
     L.ht_fsc_of_z.argtypes = [_P, dbl, C.POINTER(dbl)]
     L.ht_smooth_window.restype = C.c_int
     L.ht_smooth_window.argtypes = [_P, _P, _P, C.c_int, dbl, dbl, C.c_int, _P]
+    L.ht_smooth_filter.restype = C.c_int
+    L.ht_smooth_filter.argtypes = [_P, _P, _P, C.c_int, C.c_int, dbl, dbl, C.c_int, _P]
     L.ht_peakfind_filter.restype = C.c_int
     L.ht_peakfind_filter.argtypes = [_P, _P, _P, _P, C.c_int, C.c_int, C.c_float, i32, i64,
                                      C.POINTER(HtPeaks), _P]

@@ -17,7 +17,7 @@ LIB = os.path.join(HERE, "libhuntian_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "-shared",
-         "-cudart", "shared", "-I", os.path.join(ROOT, "include")]
+         "-cudart", "shared", "-I", os.path.join(ROOT, "include"), "-lcufft"]
 
 
 def sources():

@@ -214,9 +214,11 @@ static double host_interp(const ht_ctx* c, double x, double y, double z) {
 }
 
 static void free_ctx(ht_ctx* c) {
+    if (c->fft_n) cufftDestroy(c->fft_plan);
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt,
-                    c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_queue, c->d_stats};
+                    c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_queue,
+                    c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;

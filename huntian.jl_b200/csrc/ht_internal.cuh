@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cufft.h>
 #include <stdint.h>
 
 #include <string>
@@ -56,6 +57,10 @@ struct ht_ctx {
     size_t scratch_bytes = 0;
     void* d_win = nullptr;         // smoothing-window table
     size_t win_bytes = 0;
+    void* d_cwork = nullptr;       // complex buffer of the per-filter smoothing
+    size_t cwork_bytes = 0;
+    cufftHandle fft_plan = 0;      // C2R plan for fft_n^3 (0 = none)
+    int fft_n = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked
 

@@ -5,7 +5,10 @@
 // is evaluated once per distinct integer ix^2 + iy^2 + iz^2 into a table (first kernel)
 // and the modes are multiplied by Float32(W) from it (second kernel, bandwidth-bound:
 // 8 B read + 8 B written per mode).  k = 0 is left unchanged, as in the reference.
+#include <cufft.h>
 #include <math.h>
+
+#include <string>
 
 #include "ht_internal.cuh"
 
@@ -89,5 +92,78 @@ extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void*
                                                           (const float*)ctx->d_win);
     HT_CUDA_TRY(cudaGetLastError(), "window_apply_kernel launch");
     ctx->last_kernels = 2;
+    return HT_OK;
+}
+
+// ------------------------------------------------- window + inverse FFT + wrap ----
+//
+// ht_smooth_filter: the whole per-filter smoothing of a periodic n^3 box, delivered as the
+// tile the peak scan reads: the window above into a context-owned complex buffer, an
+// in-place cuFFT C2R (plan cached per n; the result is the padded real layout with rows of
+// 2 (n/2 + 1) floats), then one kernel that writes tile cell (i, j, k) =
+// box((i - nbuff) mod n, ...) / n^3 -- the normalisation of Julia's irfft -- for the
+// (n + 2 nbuff)^3 tile with periodic wrap.
+
+namespace {
+
+__global__ void __launch_bounds__(256) wrap_pad_kernel(const float* __restrict__ box, int n,
+                                                       long long row, int nbuff,
+                                                       float* __restrict__ tile, float scale) {
+    const int nt = n + 2 * nbuff;
+    const long long total = (long long)nt * nt * nt;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
+         c += stride) {
+        const int i = (int)(c % nt);
+        const long long r = c / nt;
+        const int j = (int)(r % nt);
+        const int k = (int)(r / nt);
+        int bi = i - nbuff, bj = j - nbuff, bk = k - nbuff;
+        bi = bi < 0 ? bi + n : (bi >= n ? bi - n : bi);
+        bj = bj < 0 ? bj + n : (bj >= n ? bj - n : bj);
+        bk = bk < 0 ? bk + n : (bk >= n ? bk - n : bk);
+        tile[c] = __ldg(box + ((long long)bk * n + bj) * row + bi) * scale;
+    }
+}
+
+}  // namespace
+
+extern "C" HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, int n,
+                                       int nbuff, double boxsize, double Rf, int wsmooth,
+                                       void* stream) {
+    if (!ctx || !d_delta_k || !d_tile) return ht_fail(HT_ERR_INVALID, "ht_smooth_filter: NULL argument");
+    if (n < 2 || n > 4096 || nbuff < 0 || nbuff > n)
+        return ht_fail(HT_ERR_INVALID, "ht_smooth_filter: need 2 <= n <= 4096 and 0 <= nbuff <= n");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const long long nk = n / 2 + 1;
+    const size_t cbytes = (size_t)nk * n * n * 2 * sizeof(float);
+    int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
+    if (rc != HT_OK) return rc;
+    if (ctx->fft_n != n) {
+        if (ctx->fft_n) { cufftDestroy(ctx->fft_plan); ctx->fft_n = 0; }
+        if (ht_fault_injected("alloc")) return ht_fail(HT_ERR_FAULT, "injected allocation fault: cuFFT plan");
+        cufftResult r = cufftPlan3d(&ctx->fft_plan, n, n, n, CUFFT_C2R);
+        if (r != CUFFT_SUCCESS)
+            return ht_fail(HT_ERR_CUDA, "cufftPlan3d(C2R) failed with code " + std::to_string((int)r));
+        ctx->fft_n = n;
+    }
+    rc = ht_smooth_window(ctx, d_delta_k, ctx->d_cwork, n, boxsize, Rf, wsmooth, stream);
+    if (rc != HT_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cufftSetStream(ctx->fft_plan, st) != CUFFT_SUCCESS)
+        return ht_fail(HT_ERR_CUDA, "cufftSetStream failed");
+    cufftResult r = cufftExecC2R(ctx->fft_plan, (cufftComplex*)ctx->d_cwork, (cufftReal*)ctx->d_cwork);
+    if (r != CUFFT_SUCCESS)
+        return ht_fail(HT_ERR_CUDA, "cufftExecC2R failed with code " + std::to_string((int)r));
+    const int nt = n + 2 * nbuff;
+    const long long total = (long long)nt * nt * nt;
+    long long blocks = (total + 255) / 256;
+    const long long cap = (long long)ctx->num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    const float scale = (float)(1.0 / ((double)n * n * n));
+    wrap_pad_kernel<<<(unsigned)blocks, 256, 0, st>>>((const float*)ctx->d_cwork, n, 2 * nk,
+                                                      nbuff, d_tile, scale);
+    HT_CUDA_TRY(cudaGetLastError(), "wrap_pad_kernel launch");
+    ctx->last_kernels = 3;
     return HT_OK;
 }

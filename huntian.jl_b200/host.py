@@ -124,6 +124,21 @@ class HaloFinder:
         w = self.smooth_window(delta_k, n, boxsize, Rf, wsmooth, out=work)
         return torch.fft.irfftn(w, s=(n, n, n), dim=(0, 1, 2)).contiguous()
 
+    def smooth_tile(self, delta_k: torch.Tensor, n: int, nbuff: int, boxsize: float,
+                    Rf: float, wsmooth: int, out: Optional[torch.Tensor] = None,
+                    stream=None) -> torch.Tensor:
+        """ht_smooth_filter: window + cuFFT inverse rfft of the periodic n^3 box, returned
+        as the (n + 2 nbuff)^3 tile with periodic wrap (float32)."""
+        if delta_k.dtype != torch.complex64 or tuple(delta_k.shape) != (n, n, n // 2 + 1):
+            raise ValueError("delta_k must be the complex64 rfft of an n^3 box")
+        nt = n + 2 * nbuff
+        out = torch.empty((nt, nt, nt), dtype=torch.float32, device=delta_k.device) \
+            if out is None else out
+        check(_lib.load().ht_smooth_filter(self._h, delta_k.contiguous().data_ptr(),
+                                           out.data_ptr(), int(n), int(nbuff), float(boxsize),
+                                           float(Rf), int(wsmooth), _stream_handle(stream)))
+        return out
+
     # ---------------------------------------------------------------- peaks ----
     def peakfind_filter(self, delta_s: torch.Tensor, mask: torch.Tensor, nbuff: int,
                         fcrit: float, filter_idx: int, max_peaks: int, out: dict,

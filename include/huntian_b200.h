@@ -25,6 +25,7 @@
  *   ht_ctx_create       -> per-call uploads of ShellTablesGPU (ext/CUDAExt.jl:16-41), the
  *                          collapse table and the SPH table (ext/CUDAExt.jl:45-52)
  *   ht_smooth_window    -> ext/CUDAExt.jl:2831-2871 `_smooth_window_kernel!`
+ *   ht_smooth_filter    -> one filter of ext/CUDAExt.jl:2985-2999 (window + irfft)
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  */
@@ -123,6 +124,14 @@ HT_API int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const float* 
  * Replaces ext/CUDAExt.jl:2831-2871 `_smooth_window_kernel!` (Filters.jl:72-99). */
 HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int n,
                             double boxsize, double Rf, int wsmooth, void* stream);
+
+/* The per-filter smoothing of a periodic n^3 box as the tile the peak scan reads:
+ * window (as ht_smooth_window) into a context buffer, cuFFT inverse real FFT normalised by
+ * 1/n^3 (Julia's irfft), and d_tile (n + 2 nbuff)^3 Float32 column-major = the box with
+ * nbuff cells of periodic wrap on every side.  Replaces, for one filter, the copy +
+ * window + irfft of ext/CUDAExt.jl:2985-2999 (Filters.smooth_field, Filters.jl:72-99). */
+HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, int n,
+                            int nbuff, double boxsize, double Rf, int wsmooth, void* stream);
 
 /* ------------------------------------------------------------ shell collapse ---- */
 
