@@ -72,13 +72,17 @@ def _peaks_json():
 
 
 def _profile_traffic(workload):
-    """Per-launch DRAM bytes of the walk kernel from a committed ncu summary, scaled to
-    the walked cells of this run (the summary stores bytes per walked cell)."""
-    p = os.path.join(ROOT, "profiles", "walk_traffic.json")
+    """DRAM bytes per walked cell of the walk kernel from the committed ncu summary
+    (profiles/walk_traffic.txt); the caller scales it by the cells walked in this run."""
+    p = os.path.join(ROOT, "profiles", "walk_traffic.txt")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    return d.get(workload) or d.get("default")
+    vals = {}
+    for ln in open(p):
+        ln = ln.split("#")[0].split()
+        if len(ln) == 2:
+            vals[ln[0]] = float(ln[1])
+    return vals.get(workload, vals.get("default"))
 
 
 class Clocks:

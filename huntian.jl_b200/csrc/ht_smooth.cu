@@ -38,29 +38,26 @@ __global__ void window_table_kernel(float* __restrict__ tab, int nvals, double d
     tab[q] = (float)w;
 }
 
+// One thread per mode; grid (ceil((n/2+1) / 256), n, n) so that the mode's (iy, iz)
+// come from the block index instead of 64-bit division.
 __global__ void __launch_bounds__(256) window_apply_kernel(const float2* __restrict__ in,
                                                            float2* __restrict__ out, int n,
                                                            const float* __restrict__ tab) {
     const int nk = n / 2 + 1;
-    const long long total = (long long)nk * n * n;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long li = (long long)blockIdx.x * blockDim.x + threadIdx.x; li < total;
-         li += stride) {
-        const int ix = (int)(li % nk);
-        const long long rem = li / nk;
-        const int iy = (int)(rem % n);
-        const int iz = (int)(rem / n);
-        const int sy = iy <= n / 2 ? iy : iy - n;
-        const int sz = iz <= n / 2 ? iz : iz - n;
-        const int q = ix * ix + sy * sy + sz * sz;
-        float2 v = in[li];
-        if (q > 0) {
-            const float w = __ldg(tab + q);
-            v.x *= w;
-            v.y *= w;
-        }
-        out[li] = v;
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ix >= nk) return;
+    const int iy = blockIdx.y, iz = blockIdx.z;
+    const long long li = ((long long)iz * n + iy) * nk + ix;
+    const int sy = iy <= n / 2 ? iy : iy - n;
+    const int sz = iz <= n / 2 ? iz : iz - n;
+    const int q = ix * ix + sy * sy + sz * sz;
+    float2 v = __ldg(in + li);
+    if (q > 0) {
+        const float w = __ldg(tab + q);
+        v.x *= w;
+        v.y *= w;
     }
+    out[li] = v;
 }
 
 }  // namespace
@@ -68,7 +65,7 @@ __global__ void __launch_bounds__(256) window_apply_kernel(const float2* __restr
 extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int n,
                                        double boxsize, double Rf, int wsmooth, void* stream) {
     if (!ctx || !d_delta_k || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: NULL argument");
-    if (n < 2 || n > 65536) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: n out of range");
+    if (n < 2 || n > 8192) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: need 2 <= n <= 8192");
     if (!(boxsize > 0.0) || !(Rf >= 0.0))
         return ht_fail(HT_ERR_INVALID, "ht_smooth_window: boxsize must be > 0 and Rf >= 0");
     if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_smooth_window");
@@ -83,13 +80,9 @@ extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void*
     window_table_kernel<<<(nvals + 255) / 256, 256, 0, st>>>((float*)ctx->d_win, nvals, dk, Rf,
                                                              wsmooth);
     HT_CUDA_TRY(cudaGetLastError(), "window_table_kernel launch");
-    const long long total = (long long)(h + 1) * n * n;
-    long long blocks = (total + 255) / 256;
-    const long long cap = (long long)ctx->num_sms * 16;
-    if (blocks > cap) blocks = cap;
-    window_apply_kernel<<<(unsigned)blocks, 256, 0, st>>>((const float2*)d_delta_k,
-                                                          (float2*)d_out, n,
-                                                          (const float*)ctx->d_win);
+    const dim3 agrid((unsigned)((h + 1 + 255) / 256), (unsigned)n, (unsigned)n);
+    window_apply_kernel<<<agrid, 256, 0, st>>>((const float2*)d_delta_k, (float2*)d_out, n,
+                                                (const float*)ctx->d_win);
     HT_CUDA_TRY(cudaGetLastError(), "window_apply_kernel launch");
     ctx->last_kernels = 2;
     return HT_OK;
@@ -106,24 +99,21 @@ extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void*
 
 namespace {
 
-__global__ void __launch_bounds__(256) wrap_pad_kernel(const float* __restrict__ box, int n,
+// One thread per tile cell; grid (ceil(nt / 128), nt, nt): the cell's (j, k) come from
+// the block index.
+__global__ void __launch_bounds__(128) wrap_pad_kernel(const float* __restrict__ box, int n,
                                                        long long row, int nbuff,
                                                        float* __restrict__ tile, float scale) {
     const int nt = n + 2 * nbuff;
-    const long long total = (long long)nt * nt * nt;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < total;
-         c += stride) {
-        const int i = (int)(c % nt);
-        const long long r = c / nt;
-        const int j = (int)(r % nt);
-        const int k = (int)(r / nt);
-        int bi = i - nbuff, bj = j - nbuff, bk = k - nbuff;
-        bi = bi < 0 ? bi + n : (bi >= n ? bi - n : bi);
-        bj = bj < 0 ? bj + n : (bj >= n ? bj - n : bj);
-        bk = bk < 0 ? bk + n : (bk >= n ? bk - n : bk);
-        tile[c] = __ldg(box + ((long long)bk * n + bj) * row + bi) * scale;
-    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nt) return;
+    const int j = blockIdx.y, k = blockIdx.z;
+    int bi = i - nbuff, bj = j - nbuff, bk = k - nbuff;
+    bi = bi < 0 ? bi + n : (bi >= n ? bi - n : bi);
+    bj = bj < 0 ? bj + n : (bj >= n ? bj - n : bj);
+    bk = bk < 0 ? bk + n : (bk >= n ? bk - n : bk);
+    tile[((long long)k * nt + j) * nt + i] =
+        __ldg(box + ((long long)bk * n + bj) * row + bi) * scale;
 }
 
 }  // namespace
@@ -156,13 +146,10 @@ extern "C" HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float
     if (r != CUFFT_SUCCESS)
         return ht_fail(HT_ERR_CUDA, "cufftExecC2R failed with code " + std::to_string((int)r));
     const int nt = n + 2 * nbuff;
-    const long long total = (long long)nt * nt * nt;
-    long long blocks = (total + 255) / 256;
-    const long long cap = (long long)ctx->num_sms * 16;
-    if (blocks > cap) blocks = cap;
     const float scale = (float)(1.0 / ((double)n * n * n));
-    wrap_pad_kernel<<<(unsigned)blocks, 256, 0, st>>>((const float*)ctx->d_cwork, n, 2 * nk,
-                                                      nbuff, d_tile, scale);
+    const dim3 wgrid((unsigned)((nt + 127) / 128), (unsigned)nt, (unsigned)nt);
+    wrap_pad_kernel<<<wgrid, 128, 0, st>>>((const float*)ctx->d_cwork, n, 2 * nk, nbuff, d_tile,
+                                           scale);
     HT_CUDA_TRY(cudaGetLastError(), "wrap_pad_kernel launch");
     ctx->last_kernels = 3;
     return HT_OK;
