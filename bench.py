@@ -6,9 +6,10 @@
 Metric: candidate peaks per second carried through peak finding (all filters, mask
 carried) and the radial-shell collapse, for one tile per GPU (weak scaling: N GPUs run N
 independent tiles, no collective on the data path).  A step is one tile's halo-finding
-stage as run_multitile_split performs it (MultiResolution.jl:1015-1219): per filter the
-cuFFT smoothing (outside this library, as in the reference) and the library's peak scan,
-then the cell-record pack and the shell collapse of every peak in one launch.
+stage as run_multitile_split performs it (MultiResolution.jl:1015-1219) with
+peak_find_tile_gpu's smoothing (ext/CUDAExt.jl:2951-3012): one rfft of the tile, then per
+filter the window + cuFFT C2R of the tile (ht_smooth_tile) and the peak scan, then the
+cell-record pack and the shell collapse of every peak in one launch.
 
 Inputs are seeded synthetic fields (BBKS LambdaCDM, Threefry noise, 2LPT), generated on
 the device before timing; they are far larger than the 126 MB L2, so no flush is needed.
@@ -137,8 +138,8 @@ class Clocks:
 # --------------------------------------------------------------------- inputs ----
 
 def make_inputs(ht, wl, seed, device):
-    """Synthetic tile: delta, psi1, psi2 on the periodic box, wrapped to the tile, plus
-    delta_k of the box for the per-filter smoothing."""
+    """Synthetic tile: delta, psi1, psi2 on the periodic box, wrapped to the tile (one tile
+    with periodic cores, Parameters.jl:418-422)."""
     import torch
     from huntian_b200 import synth
     n, L, nbuff = wl["n"], wl["L"], wl["nbuff"]
@@ -146,13 +147,14 @@ def make_inputs(ht, wl, seed, device):
     dk = synth.gaussian_box(n, L, seed, cosmo, device)
     psi1, psi2 = synth.displacements(dk, n, L, ilpt=2)
     tile = {"delta": synth.wrap_pad(synth._irfft(dk, n), nbuff)}
+    del dk
     for nm, t in zip(("etax", "etay", "etaz"), psi1):
         tile[nm] = synth.wrap_pad(t, nbuff)
     for nm, t in zip(("eta2x", "eta2y", "eta2z"), psi2):
         tile[nm] = synth.wrap_pad(t, nbuff)
     del psi1, psi2
     torch.cuda.empty_cache()
-    return dk, tile
+    return tile
 
 
 class Workload:
@@ -169,7 +171,8 @@ class Workload:
         self.finder = ht.HaloFinder(self.nhunt, tab, *axes, device=device.index or 0)
         self.ZZon = 1.0                                   # z = 0
         self.fcrit = float(np.float32(self.finder.fsc_of_z(0.0)))
-        self.dk, self.tile = make_inputs(ht, wl, seed, device)
+        self.tile = make_inputs(ht, wl, seed, device)
+        self.boxsize = self.nt * self.alatt           # the tile is FFT'd as periodic
         self.mask = torch.zeros((self.nt,) * 3, dtype=torch.int8, device=device)
         self.max_peaks = 48_000_000 if self.n >= 1024 else 6_000_000
         self.peaks = ht.HaloFinder.alloc_peaks(self.max_peaks, device, False)
@@ -182,8 +185,7 @@ class Workload:
     def smooth(self, Rf):
         if getattr(self, "_ds", None) is None:
             self._ds = torch.empty((self.nt,) * 3, dtype=torch.float32, device=self.device)
-        return self.finder.smooth_tile(self.dk, self.n, self.nbuff, self.wl["L"], Rf, 1,
-                                       out=self._ds)
+        return self.finder.smooth_tile(self.dk, self.nt, self.boxsize, Rf, 1, out=self._ds)
 
     def step(self, ev=None):
         """One tile: peak scan over all filters, then pack + shell collapse."""
@@ -191,6 +193,9 @@ class Workload:
         self.mask.zero_()
         self.peaks["count"].zero_()
         self.peaks["found"].zero_()
+        self.dk = None
+        # once per tile; torch returns a strided view, made contiguous once here
+        self.dk = torch.fft.rfftn(self.tile["delta"], dim=(0, 1, 2)).contiguous()
         for fi, flt in enumerate(self.filters, start=1):
             ds = self.smooth(flt[2])
             if ev is not None:
@@ -200,6 +205,7 @@ class Workload:
             if ev is not None:
                 ev["pf"][fi - 1][1].record()
             del ds
+        self.dk = None
         npk = int(self.peaks["count"].item())
         self.npeaks = npk
         self.mask.zero_()                                # MultiResolution.jl:1083
@@ -312,9 +318,7 @@ def run_e2e(ht, W, args):
     result arrays and the mask) are read back."""
     import torch
     host = {k: v.cpu().pin_memory() for k, v in W.tile.items()}
-    dk_host = W.dk.cpu().pin_memory()
-    h2d = sum(t.numel() * t.element_size() for t in host.values()) + \
-        dk_host.numel() * dk_host.element_size()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
     d2h = 0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -322,7 +326,6 @@ def run_e2e(ht, W, args):
     s0.record()
     tot = 0
     for _ in range(args.e2e_steps):
-        W.dk = dk_host.to(W.device, non_blocking=True)
         for k, v in host.items():
             W.tile[k] = v.to(W.device, non_blocking=True)
         npk = W.step()
@@ -382,6 +385,7 @@ def cpu_baseline(ht, W, args, steps=1):
     t_find, nfilt = 0.0, 0
     mask = np.zeros((b, b, b), np.int8)
     c0 = W.nbuff
+    W.dk = torch.fft.rfftn(W.tile["delta"], dim=(0, 1, 2)).contiguous()
     for flt in W.filters[:: max(1, len(W.filters) // 8)]:
         ds = W.smooth(flt[2])[c0:c0 + b, c0:c0 + b, c0:c0 + b].cpu().numpy()
         t0 = time.perf_counter()
@@ -390,6 +394,7 @@ def cpu_baseline(ht, W, args, steps=1):
         nfilt += 1
         if t_find > budget * 0.3:
             break
+    W.dk = None
     per_cell = t_find / (nfilt * 128 ** 3)
     core = W.nt - 2 * W.nbuff
     find_tile = per_cell * core ** 3 * len(W.filters)

@@ -27,10 +27,12 @@ HT_MODE_BATCHED = 1
 
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
-           "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_smooth_window", "ht_smooth_filter",
+           "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_smooth_window", "ht_smooth_tile",
+           "ht_smooth_filter",
            "ht_peakfind_filter",
            "ht_fields_pack",
-           "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats")
+           "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
+           "ht_device_status")
 
 
 class HTError(RuntimeError):
@@ -57,7 +59,7 @@ class HtFields(C.Structure):
 
 class HtPeakBatch(C.Structure):
     _fields_ = [("pi", _P), ("pj", _P), ("pk", _P), ("Rf", _P), ("ir2min", _P), ("ZZon", _P),
-                ("fcrit", _P), ("npeaks", C.c_int64)]
+                ("fcrit", _P), ("npeaks", C.c_int64), ("order", _P)]
 
 
 RESULT_NAMES = ("RTHL", "Fbarx", "e_v", "p_v", "strain", "eigs", "Srb", "Sbar", "Sbar2",
@@ -66,8 +68,12 @@ RESULT_WIDTH = {"strain": 9, "eigs": 3, "Sbar": 3, "Sbar2": 3, "gradpk": 3, "gra
                 "gradpkrf": 3}
 
 
+# nullable Int32 diagnostics after the 14 result arrays
+DIAG_NAMES = ("walk_shells", "collapse_shell")
+
+
 class HtResults(C.Structure):
-    _fields_ = [(n, _P) for n in RESULT_NAMES]
+    _fields_ = [(n, _P) for n in RESULT_NAMES] + [(n, _P) for n in DIAG_NAMES]
 
 
 _lib = None
@@ -98,6 +104,8 @@ def load() -> C.CDLL:
     L.ht_fsc_of_z.argtypes = [_P, dbl, C.POINTER(dbl)]
     L.ht_smooth_window.restype = C.c_int
     L.ht_smooth_window.argtypes = [_P, _P, _P, C.c_int, dbl, dbl, C.c_int, _P]
+    L.ht_smooth_tile.restype = C.c_int
+    L.ht_smooth_tile.argtypes = [_P, _P, _P, C.c_int, dbl, dbl, C.c_int, _P]
     L.ht_smooth_filter.restype = C.c_int
     L.ht_smooth_filter.argtypes = [_P, _P, _P, C.c_int, C.c_int, dbl, dbl, C.c_int, _P]
     L.ht_peakfind_filter.restype = C.c_int
@@ -113,6 +121,8 @@ def load() -> C.CDLL:
                                           dbl, i32, _P, i32, C.POINTER(HtResults), _P]
     L.ht_last_launch_stats.restype = C.c_int
     L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+    L.ht_device_status.restype = C.c_int
+    L.ht_device_status.argtypes = [_P, C.POINTER(i32)]
     _lib = L
     return L
 

@@ -215,9 +215,11 @@ static double host_interp(const ht_ctx* c, double x, double y, double z) {
 
 static void free_ctx(ht_ctx* c) {
     if (c->fft_n) cufftDestroy(c->fft_plan);
+    if (c->tile_n) cufftDestroy(c->tile_plan);
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt,
-                    c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_queue,
+                    c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
+                    c->d_queue,
                     c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -403,5 +405,21 @@ extern "C" int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t
         if (cells_walked) *cells_walked = (int64_t)h[0];
         if (shells_walked) *shells_walked = (int64_t)h[1];
     }
+    return HT_OK;
+}
+
+extern "C" int ht_device_status(ht_ctx* ctx, int32_t* status) {
+    if (!ctx || !status) return ht_fail(HT_ERR_INVALID, "ht_device_status: NULL argument");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    HT_CUDA_TRY(cudaDeviceSynchronize(), "ht_device_status: synchronize");
+    int32_t v = 0;
+    HT_CUDA_TRY(cudaMemcpy(&v, ht_status_word(ctx), sizeof v, cudaMemcpyDeviceToHost),
+                "status read");
+    if (v != 0) {
+        const int32_t z = 0;
+        HT_CUDA_TRY(cudaMemcpy(ht_status_word(ctx), &z, sizeof z, cudaMemcpyHostToDevice),
+                    "status clear");
+    }
+    *status = v;
     return HT_OK;
 }

@@ -59,13 +59,22 @@ struct ht_ctx {
     size_t win_bytes = 0;
     void* d_cwork = nullptr;       // complex buffer of the per-filter smoothing
     size_t cwork_bytes = 0;
-    cufftHandle fft_plan = 0;      // C2R plan for fft_n^3 (0 = none)
+    cufftHandle fft_plan = 0;      // in-place C2R plan for fft_n^3 (0 = none)
     int fft_n = 0;
+    cufftHandle tile_plan = 0;     // out-of-place C2R plan, unpadded output, tile_n^3
+    int tile_n = 0;
+    void* d_order_ws = nullptr;    // BATCHED peak-order keys, indices and sort temp
+    size_t order_ws_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
-    unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked
+    unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked,
+                                            // [8] (int32) device status word
 
     int64_t last_kernels = 0;
 };
+
+// Device status word: kernels with bounded waits store a non-zero code here when a wait
+// gives up, instead of trapping; ht_device_status reads and clears it.
+inline int32_t* ht_status_word(ht_ctx* ctx) { return (int32_t*)(ctx->d_stats + 8); }
 
 // ----------------------------------------------------------------- errors ----
 

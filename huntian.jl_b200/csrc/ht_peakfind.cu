@@ -1,12 +1,21 @@
 // Peak finding on one smoothed field (PeakFind.jl:15-78 semantics) on sm_100a.
 //
 // Four launches per filter, all deterministic:
-//   1. flag  : 26-neighbour local-maximum test of every inner cell.  A CTA owns a
-//              32 (i) x 8 (j) column block and streams KZ planes in k through a
-//              3-plane shared-memory ring with a one-cell halo; every delta_s value is
-//              read from HBM once per CTA.  Survivors are compacted into a bitmap with
-//              one __ballot_sync word per (k, j, 32-cell run of i), laid out in the
-//              CPU scan order k -> j -> i.
+//   1. flag  : 26-neighbour local-maximum test of every inner cell.  On the main
+//              path a CTA owns a 32 (i) x 32 (j) column block and streams kz planes in
+//              k: the planes (40 x 34 floats with the one-cell halo, the x origin
+//              rounded down to 16 bytes) arrive by TMA (cp.async.bulk.tensor) into an
+//              8-slot shared-memory ring tracked by mbarriers, so up to 8 planes per CTA
+//              are in flight instead of one DRAM round trip per plane.  Each thread owns
+//              4 cells of a column, folds their 3 x 3 maxima of every plane into
+//              registers once (separably) and keeps the last three planes' maxima, so a
+//              slot is free as soon as all warps have read it.  The int8 mask is read only for cells that pass
+//              the height and neighbour tests (the conditions are a plain AND).  Grids
+//              whose row pitch is not a multiple of 16 bytes (n % 4 != 0) or that are
+//              narrower than the box run the same test from plain loads through a
+//              3-plane ring.  Survivors are compacted into a bitmap with one
+//              __ballot_sync word per (k, j, 32-cell run of i), laid out in the CPU
+//              scan order k -> j -> i.
 //   2. count : popcount of each segment of kSegWords bitmap words.
 //   3. scan  : one CTA turns the segment counts into absolute output slots after the
 //              peaks of earlier filters and advances the running count.
@@ -16,6 +25,11 @@
 // Result: the same peak list, in the same order, as the CPU scan, independent of
 // thread timing (the reference GPU kernel reserves slots with an atomic counter and is
 // order-nondeterministic, ext/CUDAExt.jl:2921).
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
 #include "ht_internal.cuh"
 
 namespace {
@@ -93,6 +107,167 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_kernel(const float* __restr
         mprev = mcur;
         mcur = mnext;
         ff = plane[slot_next][ty + 1][tx + 1];
+    }
+}
+
+
+// ------------------------------------------------------------- TMA flag path ----
+
+constexpr int kBoxX = 40;                  // plane box width in floats (160 B)
+constexpr int kRowsPT = 4;                 // rows of j per thread
+constexpr int kTYB = kTY * kRowsPT;        // 32 rows of j per CTA
+constexpr int kBoxY = kTYB + 2;            // 34 rows: j - 1 .. j + 32
+constexpr int kStages = 8;                 // planes in flight per CTA
+constexpr int kPlaneBytes = kBoxX * kBoxY * 4;
+constexpr int kSlotFloats = 1376;          // 5504 B per slot: 128-byte aligned slots
+constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier wait: 2 s
+static_assert(kBoxX * kBoxY <= kSlotFloats && (kSlotFloats * 4) % 128 == 0, "slot size");
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ long long global_ns() {
+    long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void tma_plane(float* dst, const CUtensorMap* tm, int x, int y,
+                                          int z, unsigned long long* bar) {
+    const unsigned b = smem_addr(bar);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(b), "r"(kPlaneBytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"(smem_addr(dst)), "l"(tm), "r"(x), "r"(y), "r"(z), "r"(b) : "memory");
+}
+
+// Wait for phase `parity` of the barrier, giving up after kWaitNs.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
+    const unsigned b = smem_addr(bar);
+    long long t0 = 0;
+    for (int it = 0;; ++it) {
+        unsigned ok;
+        asm volatile("{\n .reg .pred p;\n"
+                     " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     " selp.u32 %0, 1, 0, p;\n}"
+                     : "=r"(ok) : "r"(b), "r"(parity) : "memory");
+        if (ok) return true;
+        if (it == 0) t0 = global_ns();
+        else if ((it & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
+    }
+}
+
+// One CTA: 32 (i) x 32 (j) cells over kz planes; thread (tx, ty) owns column i = ib + tx
+// and rows j = jb + 4 ty .. jb + 4 ty + 3.  Per plane it reads 6 rows x 3 columns of the
+// staged box and forms the 3 x 3 maxima of its 4 cells separably (vertical 3-maxima
+// sharing the middle pairs, then across the 3 columns).
+__global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
+    const __grid_constant__ CUtensorMap tm, const int8_t* __restrict__ mask,
+    PfGeom g, float fcrit, int kz, uint32_t* __restrict__ bits, int32_t* __restrict__ status) {
+    __shared__ __align__(128) float ring[kStages][kSlotFloats];
+    __shared__ __align__(8) unsigned long long full[kStages];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
+    const int ib = g.nbuff + blockIdx.x * kTX;   // 0-based first i of the block
+    const int jb = g.nbuff + blockIdx.y * kTYB;
+    const int kb = g.nbuff + blockIdx.z * kz;
+    const int hi = g.n - g.nbuff;                // exclusive end of the inner range
+    const int i = ib + tx, j0 = jb + kRowsPT * ty;
+    const bool icol = i < hi;
+    const int kend = min(kb + kz, hi);
+    const int x0 = (ib - 1) & ~3;                // 16-byte aligned box origin
+    const int c0 = ib - 1 - x0 + tx;             // column of i - 1 inside the box
+    const int r0 = kRowsPT * ty;                 // box row of j0 - 1
+    const int nplanes = kend - kb + 2;           // planes kb - 1 .. kend
+    const long long n = g.n, nn = n * n;
+
+    if (tid == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_addr(&full[s])));
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    int issued = 0;
+    if (tid == 0) {
+        for (; issued < kStages && issued < nplanes; ++issued)
+            tma_plane(ring[issued], &tm, x0, jb - 1, kb - 1 + issued, &full[issued]);
+    }
+    // 3x3 maxima of the thread's 4 cells in plane q, and their centre values
+    auto fold = [&](int q, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
+        const float* pl = ring[q % kStages] + r0 * kBoxX + c0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float r[kRowsPT + 2];
+#pragma unroll
+            for (int rr = 0; rr < kRowsPT + 2; ++rr) r[rr] = pl[rr * kBoxX + c];
+            const float p1 = fmaxf(r[1], r[2]), p3 = fmaxf(r[3], r[4]);
+            const float v0 = fmaxf(r[0], p1), v1 = fmaxf(p1, r[3]);
+            const float v2 = fmaxf(r[2], p3), v3 = fmaxf(p3, r[5]);
+            if (c == 0) {
+                m[0] = v0; m[1] = v1; m[2] = v2; m[3] = v3;
+            } else {
+                m[0] = fmaxf(m[0], v0); m[1] = fmaxf(m[1], v1);
+                m[2] = fmaxf(m[2], v2); m[3] = fmaxf(m[3], v3);
+            }
+            if (c == 1) {
+#pragma unroll
+                for (int rr = 0; rr < kRowsPT; ++rr) ctr[rr] = r[rr + 1];
+            }
+        }
+    };
+    // Consume plane q: wait for it, fold it, release its slot to plane q + kStages.
+    // Returns false (uniformly across the CTA) when a wait timed out.
+    int q_now = 0;
+    auto consume = [&](int q, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
+        q_now = q;
+        const bool ok = bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1));
+        fold(q, m, ctr);
+        if (__syncthreads_or(!ok)) return false;
+        if (tid == 0 && issued < nplanes) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tma_plane(ring[issued % kStages], &tm, x0, jb - 1, kb - 1 + issued,
+                      &full[issued % kStages]);
+            ++issued;
+        }
+        return true;
+    };
+
+    float mprev[kRowsPT], mcur[kRowsPT], mnext[kRowsPT];
+    float fprev[kRowsPT], ff[kRowsPT], fnext[kRowsPT];
+    bool ok = consume(0, mprev, fprev) && consume(1, mcur, ff);
+    for (int k = kb; ok && k < kend; ++k) {
+        ok = consume(k - kb + 2, mnext, fnext);
+        if (!ok) break;
+#pragma unroll
+        for (int rr = 0; rr < kRowsPT; ++rr) {
+            const int j = j0 + rr;
+            bool peak = false;
+            if (icol && j < hi) {
+                // ff < fcrit skips; any neighbour > ff rejects (ties pass); mask == 1
+                // skips.  fmaxf ignores NaN neighbours, matching `ff < NaN == false`.
+                const float m27 = fmaxf(fmaxf(mprev[rr], mcur[rr]), mnext[rr]);
+                peak = !(ff[rr] < fcrit) && !(ff[rr] < m27);
+                if (peak) peak = __ldg(mask + (long long)i + n * j + nn * k) != 1;
+            }
+            const unsigned w = __ballot_sync(0xffffffffu, peak);
+            if (tx == 0 && j < hi) {
+                const long long row = (long long)(k - g.nbuff) * g.inner + (j - g.nbuff);
+                bits[row * g.wpr + blockIdx.x] = w;
+            }
+            mprev[rr] = mcur[rr];
+            mcur[rr] = mnext[rr];
+            ff[rr] = fnext[rr];
+        }
+    }
+    if (!ok && tid == 0) {
+        // record the timeout, then wait (bounded) for the copies still in flight
+        atomicExch(status, 1);
+        for (int q = q_now; q < issued; ++q)
+            bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1));
     }
 }
 
@@ -215,6 +390,38 @@ __global__ void __launch_bounds__(kEmitThreads) pf_emit_kernel(
     }
 }
 
+
+// cuTensorMapEncodeTiled from the driver, looked up once per process.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess && q == cudaDriverEntryPointSuccess)
+            fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    });
+    return fn;
+}
+
+// 3-D tensor map of an n^3 FP32 field with a (40, 10, 1) box; false when the field does
+// not meet TMA's rules (row pitch a multiple of 16 bytes, 16-byte aligned base) or is
+// narrower than the box, and the plain-load kernel is used instead.
+bool pf_tensor_map(CUtensorMap* tm, const float* d, int n) {
+    if (n % 4 != 0 || n < kBoxX || ((uintptr_t)d & 15u) != 0) return false;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)n};
+    const cuuint64_t strides[2] = {(cuuint64_t)n * 4, (cuuint64_t)n * n * 4};
+    const cuuint32_t box[3] = {kBoxX, kBoxY, 1};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)d, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_s,
@@ -237,9 +444,24 @@ int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_
     int64_t* segbase = (int64_t*)((char*)ctx->d_pf_ws + bits_bytes);
     int32_t* segcount = (int32_t*)(segbase + nseg);
 
-    dim3 grid1((g.inner + kTX - 1) / kTX, (g.inner + kTY - 1) / kTY, (g.inner + kKZ - 1) / kKZ);
-    pf_flag_kernel<<<grid1, dim3(kTX, kTY), 0, st>>>(d_delta_s, d_mask, g, fcrit, bits);
-    HT_CUDA_TRY(cudaGetLastError(), "pf_flag_kernel launch");
+    const unsigned gx = (unsigned)((g.inner + kTX - 1) / kTX);
+    const unsigned gy = (unsigned)((g.inner + kTY - 1) / kTY);
+    CUtensorMap tm;
+    if (pf_tensor_map(&tm, d_delta_s, n)) {
+        // planes per CTA: 64, halved while the grid would give fewer than 16 CTAs per SM
+        int kz = 64;
+        const long long want = 16LL * ctx->num_sms;
+        const unsigned gyb = (unsigned)((g.inner + kTYB - 1) / kTYB);
+        while (kz > 8 && (long long)gx * gyb * ((g.inner + kz - 1) / kz) < want) kz >>= 1;
+        dim3 grid1(gx, gyb, (unsigned)((g.inner + kz - 1) / kz));
+        pf_flag_tma_kernel<<<grid1, dim3(kTX, kTY), 0, st>>>(tm, d_mask, g, fcrit, kz, bits,
+                                                             ht_status_word(ctx));
+        HT_CUDA_TRY(cudaGetLastError(), "pf_flag_tma_kernel launch");
+    } else {
+        dim3 grid1(gx, gy, (unsigned)((g.inner + kKZ - 1) / kKZ));
+        pf_flag_kernel<<<grid1, dim3(kTX, kTY), 0, st>>>(d_delta_s, d_mask, g, fcrit, bits);
+        HT_CUDA_TRY(cudaGetLastError(), "pf_flag_kernel launch");
+    }
     pf_count_kernel<<<(unsigned)nseg, kEmitThreads, 0, st>>>(bits, g.nwords, segcount);
     HT_CUDA_TRY(cudaGetLastError(), "pf_count_kernel launch");
     pf_scan_kernel<<<1, 1024, 0, st>>>(segcount, (int)nseg, segbase, out->count, out->found,

@@ -6,7 +6,8 @@
 // results.  For each peak the group walks the shells of the r^2-sorted offset table
 // outward (the per-shell gather of ShellAnalysisGPU.jl:153-229 / ext/CUDAExt.jl:752-924):
 // each lane accumulates 13 FP32 sums per shell with Kahan compensation (delta, delta*d,
-// delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L), the lanes' partial sums
+// delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L; every product's rounding
+// error is recovered exactly with an FMA and compensated too), the lanes' partial sums
 // are combined in FP64 in a fixed order through shared memory, and the shell's profile
 // (Fbar, gradients, strain) goes to a per-group scratch slot in FP64.  The walk stops as
 // soon as every shell the post-processing reads has been gathered.  The same group then
@@ -25,6 +26,8 @@
 
 #include <mutex>
 #include <string>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "ht_internal.cuh"
 
@@ -95,6 +98,7 @@ struct WalkArgs {
     const float* ZZon;
     const float* fcrit;
     long long npeaks;
+    const int32_t* order;   // nullable processing order
 
     double alatt, wRnor, aRnor, rmax2rs;
     int nbuff;
@@ -120,6 +124,15 @@ struct Kahan {
         float t = s + y;
         c = (t - s) - y;
         s = t;
+    }
+    // x * y with its rounding error folded into the compensation: fmaf gives the exact
+    // low part e = x*y - fl(x*y), and the running sum is s - c, so c -= e (a compensated
+    // dot product in FP32, in the manner of Ogita, Rump and Oishi's Dot2).
+    __device__ __forceinline__ void add_prod(float x, float y) {
+        const float p = __fmul_rn(x, y);   // never contracted into an FMA
+        const float e = fmaf(x, y, -p);
+        add(p);
+        c -= e;
     }
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
@@ -357,7 +370,13 @@ __device__ void write_no_collapse(const WalkArgs& a, long long p, const Group& g
     if (g.t == 0) {
         o.RTHL[p] = -1.0f; o.Fbarx[p] = 0.f; o.e_v[p] = 0.f; o.p_v[p] = 0.f;
         o.Srb[p] = 0.f; o.d2F[p] = 0.f; o.zvir_half[p] = -1.0f;
+        if (o.collapse_shell) o.collapse_shell[p] = 0;
     }
+}
+
+__device__ __forceinline__ void write_walk_shells(const WalkArgs& a, long long p,
+                                                  const Group& g, int shells) {
+    if (g.t == 0 && a.out.walk_shells) a.out.walk_shells[p] = shells;
 }
 
 template <bool PACKED>
@@ -467,12 +486,13 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     const double fcrit = (double)a.fcrit[p];
     if (ci < 1 || ci > a.n1 || cj < 1 || cj > a.n2 || ck < 1 || ck > a.n3) {
         // a centre outside the tile has no cells to walk (the reference would fault)
+        write_walk_shells(a, p, g, 0);
         write_no_collapse(a, p, g);
         return;
     }
     const Bounds bd = peak_bounds(a, Rf, ir2min);
     const int m = bd.m;
-    if (m < 2) { write_no_collapse(a, p, g); return; }
+    if (m < 2) { write_walk_shells(a, p, g, 1); write_no_collapse(a, p, g); return; }
 
     // ---------------------------------------------------------------- walk ----
     float cv[8];
@@ -504,15 +524,15 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
             const float d0 = (float)o.x, d1 = (float)o.y, d2 = (float)o.z;
             ++nin;
             acc[0].add(v[0]);
-            acc[1].add(v[0] * d0); acc[2].add(v[0] * d1); acc[3].add(v[0] * d2);
-            acc[4].add(v[1] * d0); acc[5].add(v[1] * d1); acc[6].add(v[1] * d2);
+            acc[1].add_prod(v[0], d0); acc[2].add_prod(v[0], d1); acc[3].add_prod(v[0], d2);
+            acc[4].add_prod(v[1], d0); acc[5].add_prod(v[1], d1); acc[6].add_prod(v[1], d2);
             const float e0 = v[2], e1 = v[3], e2 = v[4];
-            acc[7].add(2.0f * (e0 * d0));
-            acc[8].add(2.0f * (e1 * d1));
-            acc[9].add(2.0f * (e2 * d2));
-            acc[10].add(e0 * d1 + e1 * d0);
-            acc[11].add(e0 * d2 + e2 * d0);
-            acc[12].add(e1 * d2 + e2 * d1);
+            acc[7].add_prod(2.0f * e0, d0);
+            acc[8].add_prod(2.0f * e1, d1);
+            acc[9].add_prod(2.0f * e2, d2);
+            acc[10].add_prod(e0, d1); acc[10].add_prod(e1, d0);
+            acc[11].add_prod(e0, d2); acc[11].add_prod(e2, d0);
+            acc[12].add_prod(e1, d2); acc[12].add_prod(e2, d1);
         }
         // combine the lanes in FP64, lanes 0..G-1 in order (deterministic)
         R[V_F * RP + t] = acc[0].value();
@@ -560,6 +580,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         atomicAdd(a.stats, (unsigned long long)cells_in);
         atomicAdd(a.stats + 1, (unsigned long long)s_end);
     }
+    write_walk_shells(a, p, g, s_end);
 
     // ------------------------------------------------------ post-processing ----
     // gradient at the filter scale (RadialShell.jl:466-482); when mrf = 1 the window
@@ -832,6 +853,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         o.Srb[p] = (float)Srb;
         o.d2F[p] = (float)d2F;
         o.zvir_half[p] = (float)zvir_half;
+        if (o.collapse_shell) o.collapse_shell[p] = m0f - 1;
     }
     for (int i = t; i < 9; i += G) {
         const int L = i % 3, K = i / 3;   // column-major (L, K)
@@ -861,25 +883,32 @@ __device__ void process_item(const WalkArgs& a, long long item, double* P0, doub
                              int lane) {
     const long long p0 = item * kPeaksPerItem;
     const int np = (int)min((long long)kPeaksPerItem, a.npeaks - p0);
+    long long pid[kPeaksPerItem];
     int gs[kPeaksPerItem];
     bool all_small = np == kPeaksPerItem;
     for (int k = 0; k < np; ++k) {
-        gs[k] = group_size(a, p0 + k);
+        long long p = p0 + k;
+        if (a.order) {
+            p = (long long)__ldg(a.order + p);
+            if (p < 0 || p >= a.npeaks) p = -1;   // not a peak index: skipped
+        }
+        pid[k] = p;
+        gs[k] = p >= 0 ? group_size(a, p) : 0;
         all_small = all_small && gs[k] == kSmallG;
     }
     if (all_small) {
         const int q = lane / kSmallG;
         Group g{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
-        process_peak<PACKED>(a, p0 + q, P0 + q * a.scratch_stride,
+        process_peak<PACKED>(a, pid[q], P0 + q * a.scratch_stride,
                              W + q * group_smem_doubles(kSmallG), g);
     } else {
         for (int k = 0; k < np; ++k) {
             if (gs[k] == 32) {
                 Group g{32, lane, 0, 0xffffffffu};
-                process_peak<PACKED>(a, p0 + k, P0, W, g);
-            } else if (lane < kSmallG) {
+                process_peak<PACKED>(a, pid[k], P0, W, g);
+            } else if (gs[k] == kSmallG && lane < kSmallG) {
                 Group g{kSmallG, lane, 0, (1u << kSmallG) - 1u};
-                process_peak<PACKED>(a, p0 + k, P0, W, g);
+                process_peak<PACKED>(a, pid[k], P0, W, g);
             }
             __syncwarp();
         }
@@ -916,6 +945,33 @@ __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
         }
     }
 }
+// Spatial processing order for BATCHED mode: key = (lane-group class << 60) | Morton code
+// of the 0-based (i, j, k), 20 bits per axis.  Peaks consecutive in this order sit close
+// together in the tile, so the warps walking them at the same time gather largely the
+// same cell records, which then come from L2; sorting by class first keeps items of four
+// 8-lane peaks together.  The order changes no result (outputs are indexed by peak).
+__device__ __forceinline__ unsigned long long spread3(unsigned v) {
+    unsigned long long x = v & 0xfffffu;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+
+__global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
+                                                        unsigned long long* __restrict__ keys,
+                                                        int32_t* __restrict__ idx) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= a.npeaks) return;
+    const unsigned i = (unsigned)max(a.pi[p] - 1, 0), j = (unsigned)max(a.pj[p] - 1, 0),
+                   k = (unsigned)max(a.pk[p] - 1, 0);
+    const unsigned long long cls = group_size(a, p) == kSmallG ? 0ull : 1ull;
+    keys[p] = (cls << 60) | spread3(i) | (spread3(j) << 1) | (spread3(k) << 2);
+    idx[p] = (int32_t)p;
+}
+
 // Interleaved cell records: rec[2c] = (delta, delta[k,i,j], eta x, eta y),
 // rec[2c+1] = (eta z, eta2 x, eta2 y, eta2 z).  A 32x32 (i, k) tile of the transposed
 // read is staged through shared memory so both the reads and the record writes are
@@ -988,7 +1044,7 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
     a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
     a.pi = b->pi; a.pj = b->pj; a.pk = b->pk; a.Rf = b->Rf; a.ir2min = b->ir2min;
-    a.ZZon = b->ZZon; a.fcrit = b->fcrit; a.npeaks = b->npeaks;
+    a.ZZon = b->ZZon; a.fcrit = b->fcrit; a.npeaks = b->npeaks; a.order = b->order;
     a.alatt = alatt;
     const double pi = 3.14159265358979323846;
     a.aRnor = 3.0 / alatt;                   // RadialShell.jl:296-300 with hlatt = 1
@@ -1038,6 +1094,36 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     a.scratch = ctx->d_scratch; a.scratch_stride = stride;
     a.queue = ctx->d_queue; a.dynamic = packed ? 1 : 0;
     a.stats = ctx->d_stats;
+    int nk = 0;
+    if (packed && !b->order && b->npeaks > 1) {
+        if (b->npeaks > 0x7fffffffLL)
+            return ht_fail(HT_ERR_CAPACITY, "ht_shell_analyse: more than 2^31-1 peaks in one batch");
+        const int np = (int)b->npeaks;
+        size_t temp = 0;
+        HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp, (unsigned long long*)nullptr,
+                                                    (unsigned long long*)nullptr,
+                                                    (int32_t*)nullptr, (int32_t*)nullptr, np, 0,
+                                                    61, st),
+                    "radix sort size query");
+        const size_t kb = ((size_t)np * 8 + 255) / 256 * 256;
+        const size_t ib = ((size_t)np * 4 + 255) / 256 * 256;
+        rc = ht_grow(&ctx->d_order_ws, &ctx->order_ws_bytes, 2 * kb + 2 * ib + temp,
+                     "peak-order workspace");
+        if (rc != HT_OK) return rc;
+        char* w = (char*)ctx->d_order_ws;
+        unsigned long long* k_in = (unsigned long long*)w;
+        unsigned long long* k_out = (unsigned long long*)(w + kb);
+        int32_t* v_in = (int32_t*)(w + 2 * kb);
+        int32_t* v_out = (int32_t*)(w + 2 * kb + ib);
+        void* tmp = w + 2 * kb + 2 * ib;
+        order_key_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(a, k_in, v_in);
+        HT_CUDA_TRY(cudaGetLastError(), "order_key_kernel launch");
+        HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out, np, 0,
+                                                    61, st),
+                    "radix sort of the peak order");
+        a.order = v_out;
+        nk = 1 + 3;   // key kernel + the radix sort's passes (approximate count)
+    }
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st), "queue reset");
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_stats, 0, 2 * sizeof(unsigned long long), st),
                 "stats reset");
@@ -1045,7 +1131,7 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     if (packed) walk_kernel<true><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     else walk_kernel<false><<<(unsigned)blocks, kThreads, smem, st>>>(a);
     HT_CUDA_TRY(cudaGetLastError(), "walk_kernel launch");
-    ctx->last_kernels = 1;
+    ctx->last_kernels = 1 + nk;
     return HT_OK;
 }
 // ------------------------------------------------- allocation-free entry point ----

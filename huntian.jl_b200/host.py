@@ -124,10 +124,28 @@ class HaloFinder:
         w = self.smooth_window(delta_k, n, boxsize, Rf, wsmooth, out=work)
         return torch.fft.irfftn(w, s=(n, n, n), dim=(0, 1, 2)).contiguous()
 
-    def smooth_tile(self, delta_k: torch.Tensor, n: int, nbuff: int, boxsize: float,
-                    Rf: float, wsmooth: int, out: Optional[torch.Tensor] = None,
+    def smooth_tile(self, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
+                    wsmooth: int, out: Optional[torch.Tensor] = None,
                     stream=None) -> torch.Tensor:
-        """ht_smooth_filter: window + cuFFT inverse rfft of the periodic n^3 box, returned
+        """ht_smooth_tile: one filter of peak_find_tile_gpu (ext/CUDAExt.jl:2984-2989) --
+        window (with the 1/n^3 folded in) + out-of-place cuFFT C2R of the tile's own rfft
+        straight into an n^3 float32 tile."""
+        if delta_k.dtype != torch.complex64 or tuple(delta_k.shape) != (n, n, n // 2 + 1):
+            raise ValueError("delta_k must be the complex64 rfft of an n^3 tile")
+        if not delta_k.is_contiguous():
+            raise ValueError("delta_k must be contiguous (torch.fft.rfftn returns a strided "
+                             "view on CUDA: call .contiguous() once per tile)")
+        out = torch.empty((n, n, n), dtype=torch.float32, device=delta_k.device) \
+            if out is None else out
+        check(_lib.load().ht_smooth_tile(self._h, delta_k.data_ptr(),
+                                         out.data_ptr(), int(n), float(boxsize), float(Rf),
+                                         int(wsmooth), _stream_handle(stream)))
+        return out
+
+    def smooth_box_wrapped(self, delta_k: torch.Tensor, n: int, nbuff: int, boxsize: float,
+                           Rf: float, wsmooth: int, out: Optional[torch.Tensor] = None,
+                           stream=None) -> torch.Tensor:
+        """ht_smooth_filter: window + cuFFT inverse rfft of a periodic n^3 box, returned
         as the (n + 2 nbuff)^3 tile with periodic wrap (float32)."""
         if delta_k.dtype != torch.complex64 or tuple(delta_k.shape) != (n, n, n // 2 + 1):
             raise ValueError("delta_k must be the complex64 rfft of an n^3 box")
@@ -179,23 +197,38 @@ class HaloFinder:
         self._bound = ts   # keep the caller's tensors alive while bound
 
     @staticmethod
-    def alloc_results(npeaks: int, device) -> dict:
-        return {n: torch.empty(max(npeaks, 1) * RESULT_WIDTH.get(n, 1), dtype=torch.float32,
-                               device=device) for n in RESULT_NAMES}
+    def alloc_results(npeaks: int, device, diagnostics: bool = False) -> dict:
+        """The 14 result arrays; with diagnostics also the Int32 walk_shells and
+        collapse_shell arrays."""
+        out = {n: torch.empty(max(npeaks, 1) * RESULT_WIDTH.get(n, 1), dtype=torch.float32,
+                              device=device) for n in RESULT_NAMES}
+        if diagnostics:
+            for n in _lib.DIAG_NAMES:
+                out[n] = torch.empty(max(npeaks, 1), dtype=torch.int32, device=device)
+        return out
+
+    @staticmethod
+    def _results_struct(out: dict) -> HtResults:
+        return HtResults(*[out[n].data_ptr() for n in RESULT_NAMES],
+                         *[_ptr(out.get(n)) for n in _lib.DIAG_NAMES])
 
     def analyse(self, pi, pj, pk, Rf, ir2min, ZZon, fcrit, alatt: float, *,
                 rmax2rs: float = 0.0, nbuff: int = 0, mask: Optional[torch.Tensor] = None,
                 conv: str = "gpu", mode: str = "batched", out: Optional[dict] = None,
-                stream=None) -> dict:
-        """Shell collapse of the peaks (device tensors of equal length) on the bound tile."""
+                order: Optional[torch.Tensor] = None, stream=None) -> dict:
+        """Shell collapse of the peaks (device tensors of equal length) on the bound tile.
+        order: optional int32 processing order (a permutation of the peak indices); the
+        results do not depend on it."""
         if self._bound is None:
             raise _lib.HTError(_lib.HT_ERR_STATE, "bind_fields() first")
         npk = int(pi.numel())
         if out is None:
             out = self.alloc_results(npk, pi.device)
+        if order is not None:
+            assert order.dtype == torch.int32 and order.numel() == npk and order.is_contiguous()
         b = HtPeakBatch(pi.data_ptr(), pj.data_ptr(), pk.data_ptr(), Rf.data_ptr(),
-                        ir2min.data_ptr(), ZZon.data_ptr(), fcrit.data_ptr(), npk)
-        r = HtResults(*[out[n].data_ptr() for n in RESULT_NAMES])
+                        ir2min.data_ptr(), ZZon.data_ptr(), fcrit.data_ptr(), npk, _ptr(order))
+        r = self._results_struct(out)
         check(_lib.load().ht_shell_analyse(self._h, C.byref(b), float(alatt), float(rmax2rs),
                                            int(nbuff), _ptr(mask), _CONV[conv], _MODE[mode],
                                            C.byref(r), _stream_handle(stream)))
@@ -227,6 +260,13 @@ class HaloFinder:
         k, s, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(_lib.load().ht_last_launch_stats(self._h, C.byref(k), C.byref(s), C.byref(c)))
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
+
+    def device_status(self) -> int:
+        """0 when every bounded in-kernel wait since the last call completed (synchronises
+        the device and clears the word)."""
+        v = C.c_int32()
+        check(_lib.load().ht_device_status(self._h, C.byref(v)))
+        return v.value
 
 
 # ----------------------------------------------------------- reference mirrors ----
@@ -264,16 +304,18 @@ def peak_find_tile_gpu(delta_tile, filters: Sequence, fcrits: Sequence[float], t
     mask = _dev(tile_masks_in, torch.int8, device).clone()
     boxsize = n * float(alatt)   # periodic tile: boxsize_local = n * alatt
     has_lapd = ioutshear >= 1
-    delta_k = torch.fft.rfftn(delta, dim=(0, 1, 2))
-    work = torch.empty_like(delta_k)
+    delta_k = torch.fft.rfftn(delta, dim=(0, 1, 2)).contiguous()
     out = HaloFinder.alloc_peaks(max_peaks, device, has_lapd)
+    ds = torch.empty((n, n, n), dtype=torch.float32, device=device)
+    ls = torch.empty_like(ds) if has_lapd else None
     for fi, (flt, fc) in enumerate(zip(filters, fcrits), start=1):
         Rf = float(flt[2])
-        ds = finder.smooth_field(delta_k, n, boxsize, Rf, wsmooth, work=work)
-        ls = finder.smooth_field(delta_k, n, boxsize, Rf, 3, work=work) if has_lapd else None
+        finder.smooth_tile(delta_k, n, boxsize, Rf, wsmooth, out=ds)
+        if has_lapd:
+            finder.smooth_tile(delta_k, n, boxsize, Rf, 3, out=ls)
         finder.peakfind_filter(ds, mask, nbuff, float(np.float32(fc)), fi, max_peaks, out,
                                lapd_s=ls)
-        del ds, ls
+    del ds, ls
     npk = int(out["count"].item())
     sl = lambda t: t[:npk]
     res_dev = {k: (sl(v) if v is not None and k not in ("count", "found") else v)

@@ -193,10 +193,3 @@ def wrap_pad(f: torch.Tensor, nbuff: int) -> torch.Tensor:
         return f.contiguous()
     import torch.nn.functional as F
     return F.pad(f[None, None], (nbuff,) * 6, mode="circular")[0, 0].contiguous()
-
-
-def smooth_padded(finder, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
-                  wsmooth: int, nbuff: int, work=None) -> torch.Tensor:
-    """Filters.smooth_field on the periodic box (library window + cuFFT), padded to the
-    tile."""
-    return wrap_pad(finder.smooth_field(delta_k, n, boxsize, Rf, wsmooth, work=work), nbuff)

@@ -25,7 +25,9 @@
  *   ht_ctx_create       -> per-call uploads of ShellTablesGPU (ext/CUDAExt.jl:16-41), the
  *                          collapse table and the SPH table (ext/CUDAExt.jl:45-52)
  *   ht_smooth_window    -> ext/CUDAExt.jl:2831-2871 `_smooth_window_kernel!`
- *   ht_smooth_filter    -> one filter of ext/CUDAExt.jl:2985-2999 (window + irfft)
+ *   ht_smooth_tile      -> one filter of ext/CUDAExt.jl:2985-2989 (copy + window +
+ *                          irfft of the tile's own rfft, as peak_find_tile_gpu does)
+ *   ht_smooth_filter    -> the same for a periodic box delivered as a wrapped tile
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  */
@@ -133,6 +135,15 @@ HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int
 HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, int n,
                             int nbuff, double boxsize, double Rf, int wsmooth, void* stream);
 
+/* The per-filter smoothing exactly as peak_find_tile_gpu performs it on a tile
+ * (ext/CUDAExt.jl:2951-2989): d_delta_k is the rfft of the n^3 tile itself (the tile is
+ * treated as periodic with side boxsize = n * alatt), d_out (n^3 Float32 column-major)
+ * receives irfft(W . delta_k) normalised by 1/n^3.  The window (W/n^3, FP64, rounded to
+ * FP32 once) goes into a context buffer and one out-of-place cuFFT C2R writes the
+ * unpadded tile directly (plan cached per n). */
+HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                          double boxsize, double Rf, int wsmooth, void* stream);
+
 /* ------------------------------------------------------------ shell collapse ---- */
 
 /* Tile fields (device, Float32 column-major n1*n2*n3).  eta2* may all be NULL (1LPT:
@@ -169,6 +180,12 @@ typedef struct {
     const float* ZZon;
     const float* fcrit;
     int64_t npeaks;
+    /* Nullable: the order in which to process the peaks, a permutation of 0..npeaks-1
+     * (entries outside that range are skipped).  Results stay indexed by peak, so any
+     * order gives identical results.  NULL: batch order (PLAIN), or a spatial order
+     * computed by the library (BATCHED: Morton order of (i, j, k) within each lane-group
+     * class, so that concurrently walked peaks share cells in L2). */
+    const int32_t* order;
 } ht_peak_batch;
 
 /* Per-peak outputs (device, Float32; vectors are (3, npeaks) and strain (3, 3, npeaks)
@@ -189,6 +206,11 @@ typedef struct {
     float* gradpkrf;
     float* d2F;
     float* zvir_half;
+    /* Nullable diagnostics (no reference counterpart), Int32 per peak: the number of
+     * shells the gather walked (the exact early-exit point), and the shell mp* whose
+     * barrier crossing set RTHL (0 for no collapse). */
+    int32_t* walk_shells;
+    int32_t* collapse_shell;
 } ht_results;
 
 /* Radial-shell collapse of every peak of `batch` on the bound tile.  alatt in Mpc/h;
@@ -228,6 +250,13 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
  * the total number of shells walked (for the roofline's algorithmic bytes). */
 HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
                          int64_t* cells_walked);
+
+/* Device status of the context since the last call (no reference counterpart: the
+ * reference kernels have no waits).  Synchronises the device, then returns 0 in *status
+ * when every bounded wait of this context's kernels completed, or 1 when a pipeline wait
+ * of the peak scan gave up after 2 s (that filter's peaks are then incomplete); the word
+ * is cleared on read. */
+HT_API int ht_device_status(ht_ctx* ctx, int32_t* status);
 
 #ifdef __cplusplus
 }

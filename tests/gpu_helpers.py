@@ -23,7 +23,7 @@ def gpu_find_peaks(ht, finder, fields_s, mask, nbuff, fcrits, max_peaks=1 << 20,
 
 
 def run_shell(finder, fields, peaks, alatt, *, Rf, ir2min, ZZon, fcrit, nbuff=0, mask=None,
-              conv="gpu", mode="batched"):
+              conv="gpu", mode="batched", order=None, diagnostics=False):
     """fields: dict of numpy (n,n,n) arrays (delta, etax.., eta2x.., lapd optional);
     peaks: (i, j, k) 1-based arrays.  Returns dict of numpy results and the mask."""
     dev = {k: (to_dev(v) if v is not None else None) for k, v in fields.items()}
@@ -32,19 +32,23 @@ def run_shell(finder, fields, peaks, alatt, *, Rf, ir2min, ZZon, fcrit, nbuff=0,
     npk = len(peaks[0])
     b = lambda v, dt: to_dev(np.broadcast_to(np.asarray(v), (npk,)), dt)
     mask_d = to_dev(mask, torch.int8) if mask is not None else None
+    out = finder.alloc_results(npk, "cuda", diagnostics=diagnostics)
+    order_d = to_dev(order, torch.int32) if order is not None else None
     out = finder.analyse(b(peaks[0], torch.int32), b(peaks[1], torch.int32),
                          b(peaks[2], torch.int32), b(Rf, torch.float64),
                          b(ir2min, torch.int32), b(ZZon, torch.float32),
                          b(fcrit, torch.float32), alatt, nbuff=nbuff, mask=mask_d,
-                         conv=conv, mode=mode)
+                         conv=conv, mode=mode, out=out, order=order_d)
     torch.cuda.synchronize()
     res = {k: v.cpu().numpy() for k, v in out.items()}
     for k in ("strain",):
         res[k] = res[k][:9 * npk].reshape(npk, 9)
     for k in ("eigs", "Sbar", "Sbar2", "gradpk", "gradpkf", "gradpkrf"):
         res[k] = res[k][:3 * npk].reshape(npk, 3)
-    for k in ("RTHL", "Fbarx", "e_v", "p_v", "Srb", "d2F", "zvir_half"):
-        res[k] = res[k][:npk]
+    for k in ("RTHL", "Fbarx", "e_v", "p_v", "Srb", "d2F", "zvir_half", "walk_shells",
+              "collapse_shell"):
+        if k in res:
+            res[k] = res[k][:npk]
     return res, (mask_d.cpu().numpy() if mask_d is not None else None)
 
 

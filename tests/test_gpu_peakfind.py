@@ -77,11 +77,27 @@ def _smooth_random(n, seed, radii):
     return out
 
 
-@pytest.mark.parametrize("n,nbuff", [(48, 4), (45, 3), (70, 1), (37, 5)])
+# n % 4 == 0 and n >= 40 take the TMA plane ring (48, 64, 132, 136); the others the
+# plain-load ring.  132 and 136 span several k-chunks per column.
+@pytest.mark.parametrize("n,nbuff", [(48, 4), (45, 3), (70, 1), (37, 5), (64, 1), (132, 2),
+                                     (136, 4)])
 def test_random_fields_mask_carried(ht, oracle, finder, n, nbuff):
     fields = _smooth_random(n, n + nbuff, [4.0, 2.5, 1.5, 1.0])
     g = _both(ht, oracle, finder, fields, nbuff, [1.0, 1.2, 0.5, 0.0])
     assert len(g["i"]) > 20
+
+
+def test_nan_cells(ht, oracle, finder):
+    """NaN neighbours never reject a peak, and a NaN centre is a peak unless masked:
+    `ff < fcrit` and `neighbour > ff` are both false when NaN is involved
+    (PeakFind.jl:40-60)."""
+    for n in (40, 41):
+        f = _smooth_random(n, 9, [1.5])[0]
+        rng = np.random.default_rng(n)
+        idx = tuple(rng.integers(0, n, size=(3, 60)))
+        f[idx] = np.nan
+        _both(ht, oracle, finder, [f], 2, [0.3])
+    assert finder.device_status() == 0
 
 
 def test_truncation_across_filters(ht, oracle, finder):
@@ -138,7 +154,7 @@ def test_smoothing_window(ht, finder, wsmooth):
     assert got[0, 0, 0] == ak[0, 0, 0]
 
 
-def test_smooth_tile_matches_torch(ht, finder):
+def test_smooth_box_wrapped_matches_torch(ht, finder):
     """ht_smooth_filter (window + cuFFT C2R + periodic wrap) vs torch irfftn + wrap."""
     import torch
     import torch.nn.functional as F
@@ -146,10 +162,39 @@ def test_smooth_tile_matches_torch(ht, finder):
     rng = np.random.default_rng(9)
     a = torch.as_tensor(rng.standard_normal((n, n, n)).astype(np.float32), device="cuda")
     ak = torch.fft.rfftn(a, dim=(0, 1, 2)).contiguous()
-    got = finder.smooth_tile(ak, n, nb, box, Rf, 1)
+    got = finder.smooth_box_wrapped(ak, n, nb, box, Rf, 1)
     w = finder.smooth_window(ak, n, box, Rf, 1)
     ref = torch.fft.irfftn(w, s=(n, n, n), dim=(0, 1, 2))
     ref = F.pad(ref[None, None], (nb,) * 6, mode="circular")[0, 0]
     torch.cuda.synchronize()
     assert got.shape == ref.shape
     assert torch.allclose(got, ref, rtol=1e-5, atol=1e-6 * float(ref.abs().max()))
+
+
+@pytest.mark.parametrize("n,wsmooth", [(36, 1), (40, 0), (30, 3)])
+def test_smooth_tile_matches_fp64(ht, finder, n, wsmooth):
+    """ht_smooth_tile (window with 1/n^3 folded in + out-of-place C2R into the unpadded
+    tile) vs numpy FP64 irfftn of the FP64-windowed rfft: the tile smoothing of
+    peak_find_tile_gpu (ext/CUDAExt.jl:2951-2989), boxsize = n * alatt."""
+    import torch
+    alatt, Rf = 1.9, 5.0
+    box = n * alatt
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n, n)).astype(np.float32)
+    ak = torch.fft.rfftn(torch.as_tensor(a, device="cuda"), dim=(0, 1, 2)).contiguous()
+    got = finder.smooth_tile(ak, n, box, Rf, wsmooth).cpu().numpy()
+    akh = ak.cpu().numpy().astype(np.complex128)
+    dk = 2 * np.pi / box
+    kz = np.fft.fftfreq(n, 1.0 / n) * dk
+    kx = np.arange(n // 2 + 1) * dk
+    k2 = kz[:, None, None] ** 2 + kz[None, :, None] ** 2 + kx[None, None, :] ** 2
+    x = np.sqrt(k2) * Rf
+    with np.errstate(invalid="ignore", divide="ignore"):
+        w = {0: np.exp(-x * x / 8), 3: np.exp(-x * x / 8) * k2}.get(
+            wsmooth, 3 * (np.sin(x) - x * np.cos(x)) / x ** 3)
+    w = np.where(k2 == 0, 1.0, w)
+    ref = np.fft.irfftn(akh * w, s=(n, n, n))
+    scale = np.abs(ref).max()
+    assert got.shape == (n, n, n) and got.dtype == np.float32
+    # FP32 FFT round-off: a few ulp of the field's range
+    assert np.abs(got - ref).max() <= 2e-6 * scale * np.log2(n ** 3)

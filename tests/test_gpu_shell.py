@@ -144,6 +144,50 @@ def test_modes_bitwise_identical(ht, oracle, julia_table_path):
     assert np.array_equal(outs[0][1], outs[1][1])
 
 
+def test_processing_order_and_diagnostics(ht, oracle, julia_table_path):
+    """Any processing order gives bit-identical results: PLAIN (batch order), BATCHED with
+    the library's spatial order, BATCHED with a caller's random permutation.  The
+    diagnostics agree across orders; collapse_shell brackets RTHL in radius."""
+    rng = np.random.default_rng(77)
+    n = 56
+    centers = [(rng.integers(8, n - 7), rng.integers(8, n - 7), rng.integers(8, n - 7),
+                1.5 + 2.0 * rng.random(), 10.0 + 20.0 * rng.random()) for _ in range(40)]
+    d = _bump_field(n, centers, rng, noise=0.1)
+    eta = [(0.3 * rng.standard_normal(d.shape)).astype(np.float32) for _ in range(6)]
+    lapd = (0.05 * rng.standard_normal(d.shape)).astype(np.float32)
+    i, j, k, _ = oracle.find_peaks(d, np.zeros(d.shape, np.int8), 2, 0.3)
+    npk = len(i)
+    assert npk > 40
+    tab, axes = ht.read_homeltab(julia_table_path)
+    finder = ht.HaloFinder(12, tab, *axes)
+    f = _fields(d, eta[:3], eta[3:], lapd)
+    # mixed filter radii so that both lane-group sizes occur
+    Rf = np.where(np.arange(npk) % 3 == 0, 9.0, 2.5)
+    ir2 = np.array([ht.ir2min_of(r, 1.2) for r in Rf], np.int32)
+    runs = []
+    for mode, order in (("plain", None), ("batched", None),
+                        ("batched", rng.permutation(npk).astype(np.int32))):
+        r, m = run_shell(finder, f, (i, j, k), 1.2, Rf=Rf, ir2min=ir2, ZZon=1.0, fcrit=1.3,
+                         nbuff=2, mask=np.zeros(d.shape, np.int8), mode=mode, order=order,
+                         diagnostics=True)
+        runs.append((r, m))
+    for r, m in runs[1:]:
+        for key in runs[0][0]:
+            assert np.array_equal(runs[0][0][key].view(np.int32), r[key].view(np.int32)), key
+        assert np.array_equal(runs[0][1], m)
+    r = runs[0][0]
+    rad = np.sqrt(finder.shell_r2().astype(np.float64))   # rad[m - 1] of shell m
+    col = r["RTHL"] > 0
+    assert col.any() and (~col).any()
+    assert np.all(r["collapse_shell"][~col] == 0)
+    cs = r["collapse_shell"][col]
+    assert np.all(cs >= 1)
+    R = r["RTHL"][col].astype(np.float64)
+    assert np.all(R >= rad[cs - 1] * (1 - 1e-6)) and np.all(R <= rad[cs] * (1 + 1e-6))
+    assert np.all(r["walk_shells"][col] >= cs + 1)
+    assert np.all(r["walk_shells"] >= 1)
+
+
 def test_edge_peaks_near_tile_boundary(ht, oracle, julia_table_path):
     """Peaks whose shells leave the tile: out-of-tile cells are skipped, never wrapped."""
     rng = np.random.default_rng(11)
