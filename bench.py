@@ -291,7 +291,7 @@ def run_ours(args, rank, world, device):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32 sums (Kahan) + f64 collapse",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 sums + collapse",
         "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
         "config": {"workload": args.workload, "desc": W.wl["desc"], "mode": args.mode,
                    "peaks_per_step": W.npeaks, "nhunt": W.nhunt, "nshells": W.finder.nshells,

@@ -217,7 +217,7 @@ static void free_ctx(ht_ctx* c) {
     if (c->fft_n) cufftDestroy(c->fft_plan);
     if (c->tile_n) cufftDestroy(c->tile_plan);
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
-                    c->d_wrow, c->d_wm1, c->d_wwt,
+                    c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
                     c->d_queue,
                     c->d_stats};
@@ -266,6 +266,9 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
     std::vector<int32_t> wrow, wm1;
     std::vector<double> wwt;
     build_weights(rad, c->nshells, akk, wrow, wm1, wwt);
+    std::vector<double> irad(rad.size(), 0.0), irad3(rad.size(), 0.0);
+    for (size_t m = 0; m < rad.size(); ++m)
+        if (rad[m] > 0.0) { irad[m] = 1.0 / rad[m]; irad3[m] = 1.0 / (rad[m] * rad[m] * rad[m]); }
     c->nweights = (int64_t)wm1.size();
     if (const char* v = getenv("HT_SMALL_MAX_SHELLS")) c->small_max_shells = atoi(v);
     int rc;
@@ -274,6 +277,8 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
         (rc = upload(&c->d_count, c->h_count.data(), c->h_count.size(), "shell counts")) ||
         (rc = upload(&c->d_r2, c->h_r2.data(), c->h_r2.size(), "shell r2")) ||
         (rc = upload(&c->d_rad, rad.data(), rad.size(), "shell radii")) ||
+        (rc = upload(&c->d_irad, irad.data(), irad.size(), "inverse shell radii")) ||
+        (rc = upload(&c->d_irad3, irad3.data(), irad3.size(), "inverse cubed radii")) ||
         (rc = upload(&c->d_ct, c->h_ct.data(), c->h_ct.size(), "collapse table")) ||
         (rc = upload(&c->d_akk, akk.data(), akk.size(), "SPH table")) ||
         (rc = upload(&c->d_wrow, wrow.data(), wrow.size(), "weight rows")) ||

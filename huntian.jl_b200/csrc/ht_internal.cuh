@@ -28,6 +28,10 @@ struct ht_ctx {
     int32_t* d_count = nullptr;    // [nshells + 2]
     int32_t* d_r2 = nullptr;       // [nshells + 2]
     double* d_rad = nullptr;       // sqrt(r2), [nshells + 2]
+    double* d_irad = nullptr;      // 1 / rad (0 at the centre), [nshells + 2]
+    double* d_irad3 = nullptr;     // 1 / rad^3, [nshells + 2]
+    int2* d_cell = nullptr;        // (linear offset in the bound tile, char4 bits) per cell
+    int cell_n1 = 0, cell_n2 = 0;  // tile dims d_cell was built for (0: none)
     // SPH window weights of kernel_strain (RadialShell.jl:225-274), which depend only on
     // the two shell radii: row mp holds entries [wrow[mp], wrow[mp+1]) of (m1, weight)
     int64_t nweights = 0;

@@ -5,11 +5,11 @@
 // peak's own filter radius and ir2min, so every execution mode gives bit-identical
 // results.  For each peak the group walks the shells of the r^2-sorted offset table
 // outward (the per-shell gather of ShellAnalysisGPU.jl:153-229 / ext/CUDAExt.jl:752-924):
-// each lane accumulates 13 FP32 sums per shell with Kahan compensation (delta, delta*d,
-// delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L; every product's rounding
-// error is recovered exactly with an FMA and compensated too), the lanes' partial sums
-// are combined in FP64 in a fixed order through shared memory, and the shell's profile
-// (Fbar, gradients, strain) goes to a per-group scratch slot in FP64.  The walk stops as
+// each lane accumulates 13 sums per shell in FP64 from the FP32 cell values (delta,
+// delta*d, delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L, every product
+// exact in FP64); the lanes' partial sums are combined in FP64 in a fixed order through
+// shared memory, and the shell's profile (Fbar, gradients, strain) goes to a per-group
+// scratch slot in FP64.  The walk stops as
 // soon as every shell the post-processing reads has been gathered.  The same group then
 // runs the post-processing of RadialShell.jl:449-859 / ext/CUDAExt.jl:1213-1912 in FP64:
 // fcrit crossing, the inward strain/eigen/barrier walk (G steps evaluated at once, one per
@@ -23,6 +23,7 @@
 //   BATCHED reads 32-byte interleaved cell records (one sector per cell) built by
 //           pack_kernel, persistent grid with a dynamic work queue.
 #include <math.h>
+#include <string.h>
 
 #include <mutex>
 #include <string>
@@ -76,10 +77,14 @@ struct WalkArgs {
     long long s2;
 
     const char4* off;
+    const int2* cell;       // nullable: (linear offset n1-n2-n3 of the bound tile, char4 bits)
+    int nhunt;              // largest |d| of any table offset
     const int32_t* start;
     const int32_t* count;
     const int32_t* r2;
     const double* rad;
+    const double* irad;     // 1 / rad (0 for the centre shell)
+    const double* irad3;    // 1 / rad^3
     int nshells;
     const int32_t* wrow;   // SPH weight table: row mp = entries [wrow[mp], wrow[mp+1])
     const int32_t* wm1;
@@ -99,8 +104,10 @@ struct WalkArgs {
     const float* fcrit;
     long long npeaks;
     const int32_t* order;   // nullable processing order
+    const int4* bounds;     // nullable per-peak Bounds (m, m0_init, mrf, need_rf)
 
     double alatt, wRnor, aRnor, rmax2rs;
+    double zh_frac[10];     // cbrt(0.5 + 0.5 jj / 9), jj = 0..9 (zvir_half radii)
     int nbuff;
     int conv;
     int small_max_shells;   // peaks whose minimum walk is <= this use G = 8
@@ -116,25 +123,18 @@ struct WalkArgs {
 
 // ------------------------------------------------------------ small helpers ----
 
-struct Kahan {
-    float s, c;
-    __device__ __forceinline__ void zero() { s = 0.f; c = 0.f; }
-    __device__ __forceinline__ void add(float x) {
-        float y = x - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    // x * y with its rounding error folded into the compensation: fmaf gives the exact
-    // low part e = x*y - fl(x*y), and the running sum is s - c, so c -= e (a compensated
-    // dot product in FP32, in the manner of Ogita, Rump and Oishi's Dot2).
+// Per-lane FP64 accumulator.  The gathered values are FP32 and the offsets small
+// integers, so every product below is exact in FP64 and each step rounds once; the gather
+// is latency bound, so the FP64 pipe has room for it (FP32 Kahan sums were measured to
+// leave up to 4e-6 relative error on ill-conditioned strain traces, which FP64 removes).
+struct Acc {
+    double s;
+    __device__ __forceinline__ void zero() { s = 0.0; }
+    __device__ __forceinline__ void add(float x) { s += (double)x; }
     __device__ __forceinline__ void add_prod(float x, float y) {
-        const float p = __fmul_rn(x, y);   // never contracted into an FMA
-        const float e = fmaf(x, y, -p);
-        add(p);
-        c -= e;
+        s = fma((double)x, (double)y, s);
     }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+    __device__ __forceinline__ double value() const { return s; }
 };
 
 // Largest m in [lo, hi] with rad[m] < x, or lo - 1 if none (rad ascending).
@@ -171,9 +171,6 @@ __device__ __forceinline__ int first_above(const double* rad, int lo, int hi, do
 struct Group {
     int G, t, q;
     unsigned mask;
-    __device__ __forceinline__ double shfl(double v, int src) const {
-        return __shfl_sync(mask, v, src, G);
-    }
     __device__ __forceinline__ unsigned ballot(bool p) const {
         const unsigned b = __ballot_sync(mask, p) >> (q * G);
         return G == 32 ? b : (b & ((1u << G) - 1u));
@@ -413,6 +410,39 @@ struct CellLoader<false> {
     }
 };
 
+// Gather cells [c_begin, c_end) of the r^2-sorted offset list around (ci, cj, ck): lane t
+// of the group takes cells c_begin + t + u G in order and calls f(v, offset) for the
+// in-tile ones.  Out-of-tile cells are skipped (the reference never wraps).
+template <bool PACKED, class F>
+__device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck, int c_begin,
+                                       int c_end, const Group& g, bool interior, F&& f) {
+    if (interior) {
+        // every offset of the table stays inside the tile: no bounds test, and the cell's
+        // linear offset comes precomputed with its (di, dj, dk)
+        const long long cidx = (long long)(ci - 1) + (long long)a.n1 * (cj - 1) +
+                               a.s2 * (ck - 1);
+        for (int c = c_begin + g.t; c < c_end; c += g.G) {
+            const int2 e = __ldg(a.cell + c);
+            char4 o;
+            memcpy(&o, &e.y, 4);
+            float v[8];
+            CellLoader<PACKED>::load(a, cidx + e.x, ci + o.x, cj + o.y, ck + o.z, v);
+            f(v, o);
+        }
+        return;
+    }
+    for (int c = c_begin + g.t; c < c_end; c += g.G) {
+        const char4 o = __ldg(a.off + c);
+        const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
+        if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
+        const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
+                              a.s2 * (iv3 - 1);
+        float v[8];
+        CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
+        f(v, o);
+    }
+}
+
 // mrf, the shell whose gradient is reported as gradpkrf (RadialShell.jl:449-464 for the
 // CPU convention, ShellAnalysisGPU.jl:234-254 for the GPU one): the first shell s >= 2
 // minimising |r2[s] - (Rf/alatt)^2| below 10, minus the lag of the reference counters.
@@ -469,9 +499,20 @@ __device__ __forceinline__ Bounds peak_bounds(const WalkArgs& a, double Rf, int 
 
 // G = 8 for peaks whose data-independent minimum walk (to the first shell past ir2min
 // and the window of mrf) has at most small_max_shells shells, else 32.
-__device__ __forceinline__ int group_size(const WalkArgs& a, long long p) {
-    const Bounds b = peak_bounds(a, a.Rf[p], a.ir2min[p]);
+__device__ __forceinline__ int group_size_of(const WalkArgs& a, const Bounds& b) {
     return max(b.m0_init, b.need_rf) <= a.small_max_shells ? kSmallG : 32;
+}
+
+__device__ __forceinline__ Bounds bounds_of(const WalkArgs& a, long long p) {
+    if (a.bounds) {
+        const int4 v = __ldg(a.bounds + p);
+        return Bounds{v.x, v.y, v.z, v.w};
+    }
+    return peak_bounds(a, a.Rf[p], a.ir2min[p]);
+}
+
+__device__ __forceinline__ int group_size(const WalkArgs& a, long long p) {
+    return group_size_of(a, bounds_of(a, p));
 }
 
 template <bool PACKED>
@@ -480,8 +521,6 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     const double* rad = a.rad;
     const int G = g.G, t = g.t, RP = G + 1;
     const int ci = a.pi[p], cj = a.pj[p], ck = a.pk[p];
-    const double Rf = a.Rf[p];
-    const int ir2min = a.ir2min[p];
     const double ZZon = (double)a.ZZon[p];
     const double fcrit = (double)a.fcrit[p];
     if (ci < 1 || ci > a.n1 || cj < 1 || cj > a.n2 || ck < 1 || ck > a.n3) {
@@ -490,13 +529,16 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         write_no_collapse(a, p, g);
         return;
     }
-    const Bounds bd = peak_bounds(a, Rf, ir2min);
+    const Bounds bd = bounds_of(a, p);
     const int m = bd.m;
     if (m < 2) { write_walk_shells(a, p, g, 1); write_no_collapse(a, p, g); return; }
 
     // ---------------------------------------------------------------- walk ----
     float cv[8];
     const long long cidx = (long long)(ci - 1) + (long long)a.n1 * (cj - 1) + a.s2 * (ck - 1);
+    const bool interior = a.cell && ci - 1 >= a.nhunt && ci + a.nhunt <= a.n1 &&
+                          cj - 1 >= a.nhunt && cj + a.nhunt <= a.n2 && ck - 1 >= a.nhunt &&
+                          ck + a.nhunt <= a.n3;
     CellLoader<PACKED>::load(a, cidx, ci, cj, ck, cv);
     const double Fbar1 = (double)cv[0];
     for (int i = t; i < kRec; i += G) P[kRec + i] = i == P_FBAR ? Fbar1 : 0.0;
@@ -509,18 +551,12 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     for (int s = 2; s <= m; ++s) {
         const int st = __ldg(a.start + s);
         const int cnt = __ldg(a.count + s);
-        Kahan acc[13];
+        Acc acc[13];
 #pragma unroll
         for (int i = 0; i < 13; ++i) acc[i].zero();
         int nin = 0;
-        for (int c = t; c < cnt; c += G) {
-            const char4 o = __ldg(a.off + st + c);
-            const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
-            if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
-            const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
-                                  a.s2 * (iv3 - 1);
-            float v[8];
-            CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
+        gather<PACKED>(a, ci, cj, ck, st, st + cnt, g, interior,
+                       [&](const float (&v)[8], char4 o) {
             const float d0 = (float)o.x, d1 = (float)o.y, d2 = (float)o.z;
             ++nin;
             acc[0].add(v[0]);
@@ -533,7 +569,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
             acc[10].add_prod(e0, d1); acc[10].add_prod(e1, d0);
             acc[11].add_prod(e0, d2); acc[11].add_prod(e2, d0);
             acc[12].add_prod(e1, d2); acc[12].add_prod(e2, d1);
-        }
+        });
         // combine the lanes in FP64, lanes 0..G-1 in order (deterministic)
         R[V_F * RP + t] = acc[0].value();
         R[V_N * RP + t] = (double)nin;
@@ -552,7 +588,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         const double rs = rad[s];
         const double dF = ns > 0.0 ? Fs / ns : 0.0;
         const double r3p = radp * radp * radp, r3 = rs * rs * rs;
-        const double Fbar_s = (r3p * Fbarp + 0.5 * (dFbarp + dF) * (r3 - r3p)) / r3;
+        const double Fbar_s = (r3p * Fbarp + 0.5 * (dFbarp + dF) * (r3 - r3p)) * a.irad3[s];
         const double r5 = rs * rs * rs * rs * rs;
         csrb += 0.5 * (Fbarp + Fbar_s) * (r5 - rad5p);
         double* q = P + (size_t)s * kRec;
@@ -560,7 +596,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
             double v;
             if (i == P_FBAR) v = Fbar_s;
             else if (i == P_CSRB) v = csrb;
-            else v = R[(V_G + i - P_G) * RP + G] / rs;   // G, Gf, SR rows follow in order
+            else v = R[(V_G + i - P_G) * RP + G] * a.irad[s];   // G, Gf, SR rows in order
             q[i] = v;
         }
         g.sync();
@@ -713,22 +749,15 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     double Sb[3], Sb2[3];
     {
         const int ncell = __ldg(a.start + m0f);
-        Kahan ks[6];
+        Acc ks[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) ks[i].zero();
         int nloc = 0;
-        for (int c = t; c < ncell; c += G) {
-            const char4 o = __ldg(a.off + c);
-            const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
-            if (iv1 < 1 || iv1 > a.n1 || iv2 < 1 || iv2 > a.n2 || iv3 < 1 || iv3 > a.n3) continue;
-            const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
-                                  a.s2 * (iv3 - 1);
-            float v[8];
-            CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
+        gather<PACKED>(a, ci, cj, ck, 0, ncell, g, interior, [&](const float (&v)[8], char4) {
 #pragma unroll
             for (int i = 0; i < 6; ++i) ks[i].add(v[2 + i]);
             ++nloc;
-        }
+        });
         const double nS = g.sum((double)nloc);
 #pragma unroll
         for (int L = 0; L < 3; ++L) {
@@ -745,7 +774,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     // d2F
     double d2F = 0.0;
     if (a.lapd) {
-        Kahan ks; ks.zero();
+        Acc ks; ks.zero();
         int nloc = 0;
         if (a.conv == HT_CONV_GPU) {
             // all in-tile cells of shells with r <= RTHL, centre included
@@ -809,7 +838,7 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         for (int jj0 = 0; jj0 < 10; jj0 += G) {
             const int jj = jj0 + t;   // 0-based radius index
             if (jj >= 10) continue;
-            const double rcur = RTHL * pow(jj / 9.0 * 0.5 + 0.5, 1.0 / 3.0);
+            const double rcur = RTHL * a.zh_frac[jj];
             const int mm1 = m - 1;
             int mupp_rc = 1;
             if (mm1 >= 2) {
@@ -962,14 +991,33 @@ __device__ __forceinline__ unsigned long long spread3(unsigned v) {
 
 __global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
                                                         unsigned long long* __restrict__ keys,
-                                                        int32_t* __restrict__ idx) {
+                                                        int32_t* __restrict__ idx,
+                                                        int4* __restrict__ bounds) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.npeaks) return;
+    const Bounds b = peak_bounds(a, a.Rf[p], a.ir2min[p]);
+    bounds[p] = make_int4(b.m, b.m0_init, b.mrf, b.need_rf);
+    if (!keys) return;
     const unsigned i = (unsigned)max(a.pi[p] - 1, 0), j = (unsigned)max(a.pj[p] - 1, 0),
                    k = (unsigned)max(a.pk[p] - 1, 0);
-    const unsigned long long cls = group_size(a, p) == kSmallG ? 0ull : 1ull;
+    const unsigned long long cls = group_size_of(a, b) == kSmallG ? 0ull : 1ull;
     keys[p] = (cls << 60) | spread3(i) | (spread3(j) << 1) | (spread3(k) << 2);
     idx[p] = (int32_t)p;
+}
+
+// Cell table of the bound tile: the linear offset di + n1 dj + n1 n2 dk of every table
+// offset next to its (di, dj, dk), so that interior peaks gather with one 8-byte load and
+// no bounds test per cell.
+__global__ void __launch_bounds__(256) cell_table_kernel(const char4* __restrict__ off,
+                                                         int2* __restrict__ cell,
+                                                         long long ncells, int n1,
+                                                         long long s2) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncells) return;
+    const char4 o = off[c];
+    int bits;
+    memcpy(&bits, &o, 4);
+    cell[c] = make_int2((int)(o.x + (long long)n1 * o.y + s2 * o.z), bits);
 }
 
 // Interleaved cell records: rec[2c] = (delta, delta[k,i,j], eta x, eta y),
@@ -1039,12 +1087,16 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.s2 = (long long)f.n1 * f.n2;
     a.off = ctx->d_off; a.start = ctx->d_start; a.count = ctx->d_count; a.r2 = ctx->d_r2;
     a.rad = ctx->d_rad; a.nshells = ctx->nshells;
+    a.irad = ctx->d_irad; a.irad3 = ctx->d_irad3;
+    a.cell = nullptr; a.nhunt = ctx->nhunt;
+    for (int jj = 0; jj < 10; ++jj) a.zh_frac[jj] = cbrt(jj / 9.0 * 0.5 + 0.5);
     a.wrow = ctx->d_wrow; a.wm1 = ctx->d_wm1; a.wwt = ctx->d_wwt;
     a.ct = ctx->d_ct; a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz;
     a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
     a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
     a.pi = b->pi; a.pj = b->pj; a.pk = b->pk; a.Rf = b->Rf; a.ir2min = b->ir2min;
     a.ZZon = b->ZZon; a.fcrit = b->fcrit; a.npeaks = b->npeaks; a.order = b->order;
+    a.bounds = nullptr;
     a.alatt = alatt;
     const double pi = 3.14159265358979323846;
     a.aRnor = 3.0 / alatt;                   // RadialShell.jl:296-300 with hlatt = 1
@@ -1093,36 +1145,64 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
     fill_args(a, ctx, ctx->fields, b, alatt, rmax2rs, nbuff, d_mask, conv, out);
     a.scratch = ctx->d_scratch; a.scratch_stride = stride;
     a.queue = ctx->d_queue; a.dynamic = packed ? 1 : 0;
+    // interior gather table for this tile's dims (skipped if an offset could overflow int)
+    const long long n1 = ctx->fields.n1, s2 = (long long)ctx->fields.n1 * ctx->fields.n2;
+    if ((long long)ctx->nhunt * (1 + n1 + s2) < 0x7fffffffLL) {
+        if (ctx->cell_n1 != (int)n1 || ctx->cell_n2 != ctx->fields.n2 || !ctx->d_cell) {
+            if (!ctx->d_cell) {
+                rc = ht_alloc((void**)&ctx->d_cell, (size_t)ctx->ncells * sizeof(int2),
+                              "interior cell table");
+                if (rc != HT_OK) return rc;
+            }
+            cell_table_kernel<<<(unsigned)((ctx->ncells + 255) / 256), 256, 0, st>>>(
+                ctx->d_off, ctx->d_cell, ctx->ncells, (int)n1, s2);
+            HT_CUDA_TRY(cudaGetLastError(), "cell_table_kernel launch");
+            ctx->cell_n1 = (int)n1;
+            ctx->cell_n2 = ctx->fields.n2;
+        }
+        a.cell = ctx->d_cell;
+    }
     a.stats = ctx->d_stats;
     int nk = 0;
-    if (packed && !b->order && b->npeaks > 1) {
+    if (packed && b->npeaks > 0) {
+        // per-peak walk bounds (one thread per peak, instead of binary searches inside the
+        // walk), and without a caller order the spatial processing order
         if (b->npeaks > 0x7fffffffLL)
             return ht_fail(HT_ERR_CAPACITY, "ht_shell_analyse: more than 2^31-1 peaks in one batch");
         const int np = (int)b->npeaks;
+        const bool sort = !b->order && np > 1;
         size_t temp = 0;
-        HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp, (unsigned long long*)nullptr,
-                                                    (unsigned long long*)nullptr,
-                                                    (int32_t*)nullptr, (int32_t*)nullptr, np, 0,
-                                                    61, st),
-                    "radix sort size query");
-        const size_t kb = ((size_t)np * 8 + 255) / 256 * 256;
-        const size_t ib = ((size_t)np * 4 + 255) / 256 * 256;
-        rc = ht_grow(&ctx->d_order_ws, &ctx->order_ws_bytes, 2 * kb + 2 * ib + temp,
+        if (sort)
+            HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, temp,
+                                                        (unsigned long long*)nullptr,
+                                                        (unsigned long long*)nullptr,
+                                                        (int32_t*)nullptr, (int32_t*)nullptr, np,
+                                                        0, 61, st),
+                        "radix sort size query");
+        const size_t bb = ((size_t)np * 16 + 255) / 256 * 256;
+        const size_t kb = sort ? ((size_t)np * 8 + 255) / 256 * 256 : 0;
+        const size_t ib = sort ? ((size_t)np * 4 + 255) / 256 * 256 : 0;
+        rc = ht_grow(&ctx->d_order_ws, &ctx->order_ws_bytes, bb + 2 * kb + 2 * ib + temp,
                      "peak-order workspace");
         if (rc != HT_OK) return rc;
         char* w = (char*)ctx->d_order_ws;
-        unsigned long long* k_in = (unsigned long long*)w;
-        unsigned long long* k_out = (unsigned long long*)(w + kb);
-        int32_t* v_in = (int32_t*)(w + 2 * kb);
-        int32_t* v_out = (int32_t*)(w + 2 * kb + ib);
-        void* tmp = w + 2 * kb + 2 * ib;
-        order_key_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(a, k_in, v_in);
+        int4* bounds = (int4*)w;
+        unsigned long long* k_in = sort ? (unsigned long long*)(w + bb) : nullptr;
+        unsigned long long* k_out = sort ? (unsigned long long*)(w + bb + kb) : nullptr;
+        int32_t* v_in = sort ? (int32_t*)(w + bb + 2 * kb) : nullptr;
+        int32_t* v_out = sort ? (int32_t*)(w + bb + 2 * kb + ib) : nullptr;
+        void* tmp = w + bb + 2 * kb + 2 * ib;
+        order_key_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(a, k_in, v_in, bounds);
         HT_CUDA_TRY(cudaGetLastError(), "order_key_kernel launch");
-        HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out, np, 0,
-                                                    61, st),
-                    "radix sort of the peak order");
-        a.order = v_out;
-        nk = 1 + 3;   // key kernel + the radix sort's passes (approximate count)
+        nk = 1;
+        if (sort) {
+            HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out,
+                                                        np, 0, 61, st),
+                        "radix sort of the peak order");
+            a.order = v_out;
+            nk += 3;   // the radix sort's passes (approximate count)
+        }
+        a.bounds = bounds;
     }
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_queue, 0, sizeof(int32_t), st), "queue reset");
     HT_CUDA_TRY(cudaMemsetAsync(ctx->d_stats, 0, 2 * sizeof(unsigned long long), st),

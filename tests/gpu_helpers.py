@@ -33,6 +33,8 @@ def run_shell(finder, fields, peaks, alatt, *, Rf, ir2min, ZZon, fcrit, nbuff=0,
     b = lambda v, dt: to_dev(np.broadcast_to(np.asarray(v), (npk,)), dt)
     mask_d = to_dev(mask, torch.int8) if mask is not None else None
     out = finder.alloc_results(npk, "cuda", diagnostics=diagnostics)
+    for k, v in out.items():   # poison: every entry must be written by the call
+        v.fill_(float("nan") if v.is_floating_point() else -7)
     order_d = to_dev(order, torch.int32) if order is not None else None
     out = finder.analyse(b(peaks[0], torch.int32), b(peaks[1], torch.int32),
                          b(peaks[2], torch.int32), b(Rf, torch.float64),

