@@ -181,21 +181,18 @@ class Workload:
                                   dtype=torch.int32, device=device)
         self.results = None
         self.npeaks = 0
+        self.graph = None
+        self.tuned = {}
+        if mode == "learned":
+            self.model = ht.bracket.BracketModel.load(device=device)
 
     def smooth(self, Rf):
         if getattr(self, "_ds", None) is None:
             self._ds = torch.empty((self.nt,) * 3, dtype=torch.float32, device=self.device)
         return self.finder.smooth_tile(self.dk, self.nt, self.boxsize, Rf, 1, out=self._ds)
 
-    def step(self, ev=None):
-        """One tile: peak scan over all filters, then pack + shell collapse."""
-        import torch
-        self.mask.zero_()
-        self.peaks["count"].zero_()
-        self.peaks["found"].zero_()
-        self.dk = None
-        # once per tile; torch returns a strided view, made contiguous once here
-        self.dk = torch.fft.rfftn(self.tile["delta"], dim=(0, 1, 2)).contiguous()
+    def pf_loop(self, ev=None):
+        """Per filter: window + C2R of the tile (ht_smooth_tile), then the peak scan."""
         for fi, flt in enumerate(self.filters, start=1):
             ds = self.smooth(flt[2])
             if ev is not None:
@@ -204,8 +201,45 @@ class Workload:
                                         self.max_peaks, self.peaks)
             if ev is not None:
                 ev["pf"][fi - 1][1].record()
-            del ds
-        self.dk = None
+
+    def capture_graph(self):
+        """Capture the per-filter loop (80 x [window table, window, cuFFT C2R, 4 peak-scan
+        kernels] on tile1152) once into a CUDA graph, replayed every step."""
+        self.dk = torch.empty((self.nt, self.nt, self.nt // 2 + 1), dtype=torch.complex64,
+                              device=self.device)
+        self.dk.copy_(torch.fft.rfftn(self.tile["delta"], dim=(0, 1, 2)))
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.pf_loop()          # sizes every workspace and cuFFT plan before capture
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self.pf_loop()
+        torch.cuda.synchronize()
+
+    def step(self, ev=None):
+        """One tile: peak scan over all filters, then pack + shell collapse."""
+        import torch
+        self.mask.zero_()
+        self.peaks["count"].zero_()
+        self.peaks["found"].zero_()
+        graph = getattr(self, "graph", None)
+        if graph is not None:
+            # once per tile, into the buffer the graph reads
+            self.dk.copy_(torch.fft.rfftn(self.tile["delta"], dim=(0, 1, 2)))
+            if ev is not None:
+                ev["pf"][0][0].record()
+            graph.replay()
+            if ev is not None:
+                ev["pf"][0][1].record()
+        else:
+            self.dk = None
+            # once per tile; torch returns a strided view, made contiguous once here
+            self.dk = torch.fft.rfftn(self.tile["delta"], dim=(0, 1, 2)).contiguous()
+            self.pf_loop(ev)
+            self.dk = None
         npk = int(self.peaks["count"].item())
         self.npeaks = npk
         self.mask.zero_()                                # MultiResolution.jl:1083
@@ -223,15 +257,61 @@ class Workload:
         fc = torch.full((npk,), self.fcrit, dtype=torch.float32, device=self.device)
         if self.results is None or self.results["RTHL"].numel() < npk:
             self.results = self.ht.HaloFinder.alloc_results(npk, self.device)
+        pi, pj, pk = self.peaks["i"][:npk], self.peaks["j"][:npk], self.peaks["k"][:npk]
         if ev is not None:
             ev["walk"][0].record()
-        self.finder.analyse(self.peaks["i"][:npk], self.peaks["j"][:npk],
-                            self.peaks["k"][:npk], Rf, ir2, zz, fc, self.alatt,
-                            nbuff=self.nbuff, mask=self.mask, mode=self.mode,
-                            out=self.results)
+        cost = None
+        if self.mode == "learned":
+            br = self.ht.bracket
+            F = br.features(self.finder, pi, pj, pk, Rf, ir2, zz, fc, self.alatt,
+                            peak_delta=self.peaks["delta"][:npk])
+            cost = br.predict(self.finder, self.model, F)[:, 1].contiguous()
+        self.finder.analyse(pi, pj, pk, Rf, ir2, zz, fc, self.alatt, nbuff=self.nbuff,
+                            mask=self.mask, mode=self.mode, out=self.results, cost=cost)
         if ev is not None:
             ev["walk"][1].record()
         return npk
+
+    def time_walk(self, reps=2):
+        """Walk-only timing on the current peaks (the autotuner's probe)."""
+        npk = self.npeaks
+        fidx = self.peaks["filter_idx"][:npk].long() - 1
+        args = (self.peaks["i"][:npk], self.peaks["j"][:npk], self.peaks["k"][:npk],
+                self.Rf_f[fidx], self.ir2_f[fidx],
+                torch.full((npk,), self.ZZon, dtype=torch.float32, device=self.device),
+                torch.full((npk,), self.fcrit, dtype=torch.float32, device=self.device))
+        cost = None
+        if self.mode == "learned":
+            br = self.ht.bracket
+            F = br.features(self.finder, *args, self.alatt,
+                            peak_delta=self.peaks["delta"][:npk])
+            cost = br.predict(self.finder, self.model, F)[:, 1].contiguous()
+        best = None
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            self.mask.zero_()
+            a.record()
+            self.finder.analyse(*args, self.alatt, nbuff=self.nbuff, mask=self.mask,
+                                mode=self.mode, out=self.results, cost=cost)
+            b.record()
+            torch.cuda.synchronize()
+            t = a.elapsed_time(b)
+            best = t if best is None else min(best, t)
+        return best
+
+    def autotune(self):
+        """Pick the result-neutral launch parameters by timing them on this workload: the
+        LEARNED block size (HT_TUNE_BLOCK_BITS) and the walk's blocks per SM."""
+        chosen = {}
+        if self.mode == "learned":
+            t = {b: (self.finder.tune(block_bits=b), self.time_walk())[1] for b in (15, 16, 17, 18, 19)}
+            chosen["block_bits"] = min(t, key=t.get)
+            self.finder.tune(block_bits=chosen["block_bits"])
+        t = {b: (self.finder.tune(walk_bpsm=b), self.time_walk())[1] for b in (2, 3)}
+        chosen["walk_bpsm"] = min(t, key=t.get)
+        self.finder.tune(walk_bpsm=chosen["walk_bpsm"])
+        self.tuned = chosen
+        return chosen
 
 
 def run_ours(args, rank, world, device):
@@ -240,7 +320,13 @@ def run_ours(args, rank, world, device):
     seed = args.seed + rank
     W = Workload(ht, args.workload, seed, device, args.mode)
     dist = world > 1
-    for _ in range(args.warmup):
+    W.step()
+    torch.cuda.synchronize()
+    if args.autotune:
+        W.autotune()
+    if args.graph:
+        W.capture_graph()
+    for _ in range(args.warmup - 1):
         W.step()
     torch.cuda.synchronize()
     stats = W.finder.last_stats()
@@ -264,7 +350,8 @@ def run_ours(args, rank, world, device):
     torch.cuda.synchronize()
     ck = clocks.stop() if clocks else None
     t_ms = start.elapsed_time(end)
-    pf_ms = sum(a.elapsed_time(b) for e in evs for a, b in e["pf"]) / args.steps
+    npf = nf if W.graph is None else 1    # with the graph one event pair spans the loop
+    pf_ms = sum(a.elapsed_time(b) for e in evs for a, b in e["pf"][:npf]) / args.steps
     pack_ms = sum(e["pack"][0].elapsed_time(e["pack"][1]) for e in evs) / args.steps
     walk_ms = sum(e["walk"][0].elapsed_time(e["walk"][1]) for e in evs) / args.steps
     if dist:
@@ -294,17 +381,22 @@ def run_ours(args, rank, world, device):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 sums + collapse",
         "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
         "config": {"workload": args.workload, "desc": W.wl["desc"], "mode": args.mode,
+                   "cuda_graph": bool(args.graph), "autotuned": W.tuned,
                    "peaks_per_step": W.npeaks, "nhunt": W.nhunt, "nshells": W.finder.nshells,
                    "fcrit": W.fcrit, "l2": "inputs (43 GB of fields) >> 126 MB L2, no flush",
                    "parallelism": f"tile-per-GPU x{world}"},
-        "breakdown_ms": {"peakfind_kernels": pf_ms, "pack": pack_ms, "shell_walk": walk_ms,
+        "breakdown_ms": {"peakfind_kernels" if W.graph is None else
+                         "smoothing_and_peakfind_graph": pf_ms, "pack": pack_ms,
+                         "shell_walk": walk_ms,
                          "smoothing_fft_and_rest": ms_per_step - pf_ms - pack_ms - walk_ms},
         "hot_path_peaks_per_s": W.npeaks / ((pf_ms + pack_ms + walk_ms) / 1e3),
         "roofline": {"kernel": "walk_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
                      "peak_source": peak_kind, "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes, "cells_walked": cells},
-        "gpu_launches": int(args.steps * (4 * nf + 1 + 1)),
+        # ours per step: 2 window + 4 peak-scan kernels per filter, pack, order keys, walk
+        # (+ features and MLP in learned mode); cuFFT and CUB launches not counted
+        "gpu_launches": int(args.steps * (6 * nf + 3 + (2 if args.mode == "learned" else 0))),
         "clocks": ck,
         "e2e": e2e,
     }
@@ -385,6 +477,7 @@ def cpu_baseline(ht, W, args, steps=1):
     t_find, nfilt = 0.0, 0
     mask = np.zeros((b, b, b), np.int8)
     c0 = W.nbuff
+    saved_dk = W.dk          # the CUDA graph (if any) reads this buffer: keep it alive
     W.dk = torch.fft.rfftn(W.tile["delta"], dim=(0, 1, 2)).contiguous()
     for flt in W.filters[:: max(1, len(W.filters) // 8)]:
         ds = W.smooth(flt[2])[c0:c0 + b, c0:c0 + b, c0:c0 + b].cpu().numpy()
@@ -394,7 +487,7 @@ def cpu_baseline(ht, W, args, steps=1):
         nfilt += 1
         if t_find > budget * 0.3:
             break
-    W.dk = None
+    W.dk = saved_dk
     per_cell = t_find / (nfilt * 128 ** 3)
     core = W.nt - 2 * W.nbuff
     find_tile = per_cell * core ** 3 * len(W.filters)
@@ -440,7 +533,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tile1152", choices=list(WORKLOADS))
-    ap.add_argument("--mode", default="batched", choices=["batched", "plain"])
+    ap.add_argument("--mode", default="learned", choices=["learned", "batched", "plain"])
+    ap.add_argument("--graph", type=int, default=1,
+                    help="capture the per-filter smoothing + peak-scan loop in a CUDA graph")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="time the result-neutral launch parameters once and keep the best")
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--e2e-steps", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)

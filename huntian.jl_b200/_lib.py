@@ -24,6 +24,11 @@ HT_CONV_GPU = 0
 HT_CONV_CPU = 1
 HT_MODE_PLAIN = 0
 HT_MODE_BATCHED = 1
+HT_MODE_LEARNED = 2
+HT_BRACKET_NPARAMS = 9928
+HT_TUNE_BLOCK_BITS = 1
+HT_TUNE_PF_KZ = 2
+HT_TUNE_WALK_BPSM = 3
 
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
@@ -32,7 +37,8 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_peakfind_filter",
            "ht_fields_pack",
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
-           "ht_device_status")
+           "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
+           "ht_bracket_adam", "ht_ctx_tune")
 
 
 class HTError(RuntimeError):
@@ -59,7 +65,7 @@ class HtFields(C.Structure):
 
 class HtPeakBatch(C.Structure):
     _fields_ = [("pi", _P), ("pj", _P), ("pk", _P), ("Rf", _P), ("ir2min", _P), ("ZZon", _P),
-                ("fcrit", _P), ("npeaks", C.c_int64), ("order", _P)]
+                ("fcrit", _P), ("npeaks", C.c_int64), ("order", _P), ("cost", _P)]
 
 
 RESULT_NAMES = ("RTHL", "Fbarx", "e_v", "p_v", "strain", "eigs", "Srb", "Sbar", "Sbar2",
@@ -74,6 +80,11 @@ DIAG_NAMES = ("walk_shells", "collapse_shell")
 
 class HtResults(C.Structure):
     _fields_ = [(n, _P) for n in RESULT_NAMES] + [(n, _P) for n in DIAG_NAMES]
+
+
+class HtBracketModel(C.Structure):
+    _fields_ = [(n, _P) for n in ("W1", "W2", "W3", "W4", "b1", "b2", "b3", "b4", "mean",
+                                  "istd")]
 
 
 _lib = None
@@ -123,6 +134,17 @@ def load() -> C.CDLL:
     L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
     L.ht_device_status.restype = C.c_int
     L.ht_device_status.argtypes = [_P, C.POINTER(i32)]
+    L.ht_ctx_tune.restype = C.c_int
+    L.ht_ctx_tune.argtypes = [_P, i32, i64]
+    L.ht_bracket_features.restype = C.c_int
+    L.ht_bracket_features.argtypes = [_P, C.POINTER(HtPeakBatch), _P, dbl, _P, _P]
+    L.ht_bracket_predict.restype = C.c_int
+    L.ht_bracket_predict.argtypes = [_P, C.POINTER(HtBracketModel), _P, i64, _P, _P]
+    L.ht_bracket_grad.restype = C.c_int
+    L.ht_bracket_grad.argtypes = [_P, C.POINTER(HtBracketModel), _P, _P, i64, _P, _P, _P]
+    L.ht_bracket_adam.restype = C.c_int
+    L.ht_bracket_adam.argtypes = [_P, _P, _P, _P, _P, i32, C.c_float,
+                                  C.POINTER(HtBracketModel), _P]
     _lib = L
     return L
 

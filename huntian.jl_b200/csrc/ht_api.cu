@@ -219,7 +219,7 @@ static void free_ctx(ht_ctx* c) {
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
-                    c->d_queue,
+                    c->d_mlp_ws, c->d_queue,
                     c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -387,8 +387,11 @@ extern "C" int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* b, double alat
         return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: unknown conv");
     if (conv == HT_CONV_CPU && rmax2rs > 0.0)
         return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: HT_CONV_CPU supports rmax2rs == 0 only");
-    if (mode != HT_MODE_PLAIN && mode != HT_MODE_BATCHED)
+    if (mode != HT_MODE_PLAIN && mode != HT_MODE_BATCHED && mode != HT_MODE_LEARNED)
         return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: unknown mode");
+    if (mode == HT_MODE_LEARNED && !b->order && !b->cost && b->npeaks > 0)
+        return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: HT_MODE_LEARNED needs batch->cost "
+                                       "(ht_bracket_predict) or batch->order");
     if (nbuff < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: nbuff < 0");
     if (ctx->nshells < 3) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: hunt radius too small");
     if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_shell_analyse");
@@ -427,4 +430,25 @@ extern "C" int ht_device_status(ht_ctx* ctx, int32_t* status) {
     }
     *status = v;
     return HT_OK;
+}
+
+extern "C" int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value) {
+    if (!ctx) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: ctx is NULL");
+    switch (key) {
+        case HT_TUNE_BLOCK_BITS:
+            if (value < 0 || value > 40) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: block bits must be 0..40");
+            ctx->tune_block_bits = (int)value;
+            return HT_OK;
+        case HT_TUNE_PF_KZ:
+            if (value != 0 && (value < 2 || value > 1024))
+                return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: planes per CTA must be 0 or 2..1024");
+            ctx->tune_pf_kz = (int)value;
+            return HT_OK;
+        case HT_TUNE_WALK_BPSM:
+            if (value < 0 || value > 32) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: blocks per SM must be 0..32");
+            ctx->tune_walk_bpsm = (int)value;
+            return HT_OK;
+        default:
+            return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: unknown key " + std::to_string(key));
+    }
 }

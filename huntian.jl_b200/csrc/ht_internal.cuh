@@ -40,6 +40,10 @@ struct ht_ctx {
     double* d_wwt = nullptr;
     // peaks whose minimum walk spans at most this many shells run 8 lanes per peak
     int small_max_shells = 96;
+    // result-neutral tunables (ht_ctx_tune)
+    int tune_block_bits = 17;      // LEARNED order: spatial block of 2^bits cells
+    int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)
+    int tune_walk_bpsm = 0;        // walk: blocks per SM (0: occupancy maximum)
 
     // collapse table + SPH table
     std::vector<float> h_ct;
@@ -69,6 +73,8 @@ struct ht_ctx {
     int tile_n = 0;
     void* d_order_ws = nullptr;    // BATCHED peak-order keys, indices and sort temp
     size_t order_ws_bytes = 0;
+    void* d_mlp_ws = nullptr;      // bracket training activations
+    size_t mlp_ws_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked,
                                             // [8] (int32) device status word

@@ -453,6 +453,7 @@ int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_
         const long long want = 16LL * ctx->num_sms;
         const unsigned gyb = (unsigned)((g.inner + kTYB - 1) / kTYB);
         while (kz > 8 && (long long)gx * gyb * ((g.inner + kz - 1) / kz) < want) kz >>= 1;
+        if (ctx->tune_pf_kz > 0) kz = ctx->tune_pf_kz;   // autotuned (ht_ctx_tune)
         dim3 grid1(gx, gyb, (unsigned)((g.inner + kz - 1) / kz));
         pf_flag_tma_kernel<<<grid1, dim3(kTX, kTY), 0, st>>>(tm, d_mask, g, fcrit, kz, bits,
                                                              ht_status_word(ctx));

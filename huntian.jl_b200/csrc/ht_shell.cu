@@ -111,6 +111,7 @@ struct WalkArgs {
     int nbuff;
     int conv;
     int small_max_shells;   // peaks whose minimum walk is <= this use G = 8
+    int block_bits;         // LEARNED order: Morton block of 2^block_bits cells
     int8_t* mask;
     ht_results out;
 
@@ -974,8 +975,9 @@ __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
         }
     }
 }
-// Spatial processing order for BATCHED mode: key = (lane-group class << 60) | Morton code
-// of the 0-based (i, j, k), 20 bits per axis.  Peaks consecutive in this order sit close
+// Processing order for BATCHED mode: key = (lane-group class << 60) | Morton code of the
+// 0-based (i, j, k), 20 bits per axis; in LEARNED mode the predicted cost (descending)
+// comes before the coarse Morton code.  Peaks consecutive in this order sit close
 // together in the tile, so the warps walking them at the same time gather largely the
 // same cell records, which then come from L2; sorting by class first keeps items of four
 // 8-lane peaks together.  The order changes no result (outputs are indexed by peak).
@@ -992,7 +994,8 @@ __device__ __forceinline__ unsigned long long spread3(unsigned v) {
 __global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
                                                         unsigned long long* __restrict__ keys,
                                                         int32_t* __restrict__ idx,
-                                                        int4* __restrict__ bounds) {
+                                                        int4* __restrict__ bounds,
+                                                        const float* __restrict__ cost) {
     const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= a.npeaks) return;
     const Bounds b = peak_bounds(a, a.Rf[p], a.ir2min[p]);
@@ -1001,7 +1004,18 @@ __global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
     const unsigned i = (unsigned)max(a.pi[p] - 1, 0), j = (unsigned)max(a.pj[p] - 1, 0),
                    k = (unsigned)max(a.pk[p] - 1, 0);
     const unsigned long long cls = group_size_of(a, b) == kSmallG ? 0ull : 1ull;
-    keys[p] = (cls << 60) | spread3(i) | (spread3(j) << 1) | (spread3(k) << 2);
+    const unsigned long long mort = spread3(i) | (spread3(j) << 1) | (spread3(k) << 2);
+    if (cost) {
+        // learned order: coarse spatial blocks of 2^block_bits cells (Morton prefix, keeps
+        // the L2 locality), then descending predicted cost (1/16-cell steps, 24 bits)
+        float c = cost[p];
+        c = c == c ? fminf(fmaxf(c, 0.f), 1.0e6f) : 0.f;
+        const unsigned long long q = min((unsigned long long)(c * 16.f), 0xFFFFFFull);
+        const unsigned long long blk = (mort >> a.block_bits) & ((1ull << 38) - 1);
+        keys[p] = (cls << 62) | (blk << 24) | (0xFFFFFFull - q);
+    } else {
+        keys[p] = (cls << 60) | mort;
+    }
     idx[p] = (int32_t)p;
 }
 
@@ -1103,6 +1117,7 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
     a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
     a.small_max_shells = ctx->small_max_shells;
+    a.block_bits = ctx->tune_block_bits;
     a.queue = nullptr; a.dynamic = 0; a.stats = nullptr;
 }
 
@@ -1126,10 +1141,11 @@ static int walk_blocks_per_sm(int* bpsm) {
 int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rmax2rs,
                    int32_t nbuff, int8_t* d_mask, int32_t conv, int32_t mode,
                    const ht_results* out, cudaStream_t st) {
-    const bool packed = mode == HT_MODE_BATCHED;
+    const bool packed = mode != HT_MODE_PLAIN;   // BATCHED and LEARNED
     int bpsm = 0;
     int rc = packed ? walk_blocks_per_sm<true>(&bpsm) : walk_blocks_per_sm<false>(&bpsm);
     if (rc != HT_OK) return rc;
+    if (ctx->tune_walk_bpsm > 0 && ctx->tune_walk_bpsm < bpsm) bpsm = ctx->tune_walk_bpsm;
     long long blocks = (long long)ctx->num_sms * bpsm;
     const long long items = (b->npeaks + kPeaksPerItem - 1) / kPeaksPerItem;
     const long long need = (items + kWarpsPerBlock - 1) / kWarpsPerBlock;
@@ -1177,7 +1193,7 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
                                                         (unsigned long long*)nullptr,
                                                         (unsigned long long*)nullptr,
                                                         (int32_t*)nullptr, (int32_t*)nullptr, np,
-                                                        0, 61, st),
+                                                        0, 63, st),
                         "radix sort size query");
         const size_t bb = ((size_t)np * 16 + 255) / 256 * 256;
         const size_t kb = sort ? ((size_t)np * 8 + 255) / 256 * 256 : 0;
@@ -1192,12 +1208,14 @@ int ht_launch_walk(ht_ctx* ctx, const ht_peak_batch* b, double alatt, double rma
         int32_t* v_in = sort ? (int32_t*)(w + bb + 2 * kb) : nullptr;
         int32_t* v_out = sort ? (int32_t*)(w + bb + 2 * kb + ib) : nullptr;
         void* tmp = w + bb + 2 * kb + 2 * ib;
-        order_key_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(a, k_in, v_in, bounds);
+        const float* cost = mode == HT_MODE_LEARNED ? b->cost : nullptr;
+        order_key_kernel<<<(unsigned)((np + 255) / 256), 256, 0, st>>>(a, k_in, v_in, bounds,
+                                                                        cost);
         HT_CUDA_TRY(cudaGetLastError(), "order_key_kernel launch");
         nk = 1;
         if (sort) {
             HT_CUDA_TRY(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out,
-                                                        np, 0, 61, st),
+                                                        np, 0, 63, st),
                         "radix sort of the peak order");
             a.order = v_out;
             nk += 3;   // the radix sort's passes (approximate count)

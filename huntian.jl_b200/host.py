@@ -21,11 +21,12 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import (HT_CONV_CPU, HT_CONV_GPU, HT_MODE_BATCHED, HT_MODE_PLAIN, RESULT_NAMES,
-                   RESULT_WIDTH, HtFields, HtPeakBatch, HtPeaks, HtResults, check)
+from ._lib import (HT_CONV_CPU, HT_CONV_GPU, HT_MODE_BATCHED, HT_MODE_LEARNED, HT_MODE_PLAIN,
+                   RESULT_NAMES, RESULT_WIDTH, HtFields, HtPeakBatch, HtPeaks, HtResults,
+                   check)
 
 _CONV = {"gpu": HT_CONV_GPU, "cpu": HT_CONV_CPU}
-_MODE = {"plain": HT_MODE_PLAIN, "batched": HT_MODE_BATCHED}
+_MODE = {"plain": HT_MODE_PLAIN, "batched": HT_MODE_BATCHED, "learned": HT_MODE_LEARNED}
 
 
 def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
@@ -215,10 +216,12 @@ class HaloFinder:
     def analyse(self, pi, pj, pk, Rf, ir2min, ZZon, fcrit, alatt: float, *,
                 rmax2rs: float = 0.0, nbuff: int = 0, mask: Optional[torch.Tensor] = None,
                 conv: str = "gpu", mode: str = "batched", out: Optional[dict] = None,
-                order: Optional[torch.Tensor] = None, stream=None) -> dict:
+                order: Optional[torch.Tensor] = None, cost: Optional[torch.Tensor] = None,
+                stream=None) -> dict:
         """Shell collapse of the peaks (device tensors of equal length) on the bound tile.
-        order: optional int32 processing order (a permutation of the peak indices); the
-        results do not depend on it."""
+        order: optional int32 processing order (a permutation of the peak indices); cost:
+        float32 predicted walk cost per peak for mode="learned" (bracket.predict's high
+        quantile).  Neither changes any result."""
         if self._bound is None:
             raise _lib.HTError(_lib.HT_ERR_STATE, "bind_fields() first")
         npk = int(pi.numel())
@@ -226,8 +229,11 @@ class HaloFinder:
             out = self.alloc_results(npk, pi.device)
         if order is not None:
             assert order.dtype == torch.int32 and order.numel() == npk and order.is_contiguous()
+        if cost is not None:
+            assert cost.dtype == torch.float32 and cost.numel() == npk and cost.is_contiguous()
         b = HtPeakBatch(pi.data_ptr(), pj.data_ptr(), pk.data_ptr(), Rf.data_ptr(),
-                        ir2min.data_ptr(), ZZon.data_ptr(), fcrit.data_ptr(), npk, _ptr(order))
+                        ir2min.data_ptr(), ZZon.data_ptr(), fcrit.data_ptr(), npk, _ptr(order),
+                        _ptr(cost))
         r = self._results_struct(out)
         check(_lib.load().ht_shell_analyse(self._h, C.byref(b), float(alatt), float(rmax2rs),
                                            int(nbuff), _ptr(mask), _CONV[conv], _MODE[mode],
@@ -260,6 +266,15 @@ class HaloFinder:
         k, s, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(_lib.load().ht_last_launch_stats(self._h, C.byref(k), C.byref(s), C.byref(c)))
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
+
+    def tune(self, block_bits: Optional[int] = None, pf_kz: Optional[int] = None,
+             walk_bpsm: Optional[int] = None) -> None:
+        """Set result-neutral launch parameters (ht_ctx_tune)."""
+        L = _lib.load()
+        for key, v in ((_lib.HT_TUNE_BLOCK_BITS, block_bits), (_lib.HT_TUNE_PF_KZ, pf_kz),
+                       (_lib.HT_TUNE_WALK_BPSM, walk_bpsm)):
+            if v is not None:
+                check(L.ht_ctx_tune(self._h, key, int(v)))
 
     def device_status(self) -> int:
         """0 when every bounded in-kernel wait since the last call completed (synchronises

@@ -65,6 +65,7 @@ extern "C" {
 /* shell-walk execution modes (all return identical results) */
 #define HT_MODE_PLAIN 0    /* per-field gathers, static peak-to-warp schedule */
 #define HT_MODE_BATCHED 1  /* interleaved cell records, persistent kernel, dynamic queue */
+#define HT_MODE_LEARNED 2  /* BATCHED, peaks ordered by a predicted walk length (batch cost) */
 
 typedef struct ht_ctx ht_ctx;
 
@@ -186,6 +187,11 @@ typedef struct {
      * computed by the library (BATCHED: Morton order of (i, j, k) within each lane-group
      * class, so that concurrently walked peaks share cells in L2). */
     const int32_t* order;
+    /* Nullable: predicted cost per peak (the learned bracket's high quantile of the walk's
+     * stop radius, ht_bracket_predict).  HT_MODE_LEARNED without a caller order processes
+     * the peaks by descending cost within each lane-group class, so that the peaks sharing
+     * a warp walk similar distances and the longest walks start first.  Ignored otherwise. */
+    const float* cost;
 } ht_peak_batch;
 
 /* Per-peak outputs (device, Float32; vectors are (3, npeaks) and strain (3, 3, npeaks)
@@ -245,6 +251,68 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
                                    const ht_peak_batch* batch, double alatt, double rmax2rs,
                                    int32_t nbuff, int8_t* d_mask, int32_t conv,
                                    const ht_results* out, void* stream);
+
+/* Result-neutral tunables of a context, for an autotuner (no counterpart in the
+ * reference).  None of them changes any output: they only change launch shapes and the
+ * processing order.
+ *   HT_TUNE_BLOCK_BITS  HT_MODE_LEARNED order: peaks are grouped into spatial blocks of
+ *                       2^value cells (Morton prefix) and ordered by descending predicted
+ *                       cost inside a block (default 17);
+ *   HT_TUNE_PF_KZ       peak scan: k-planes per CTA (0 = chosen from the grid size);
+ *   HT_TUNE_WALK_BPSM   shell walk: resident blocks per SM (0 = the occupancy maximum). */
+#define HT_TUNE_BLOCK_BITS 1
+#define HT_TUNE_PF_KZ 2
+#define HT_TUNE_WALK_BPSM 3
+HT_API int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value);
+
+/* ------------------------------------------------------ learned walk bracket ---- */
+
+/* A 12 -> 64 -> 64 -> 64 -> 2 MLP predicting the 10 % and 90 % quantiles of the radius at
+ * which a peak's shell walk stops, used only to order the collapse work (HT_MODE_LEARNED);
+ * results never depend on it.  No counterpart in the reference.  Device arrays: BF16
+ * weights (raw 16-bit), row-major [out][in]: W1 64x16 (inputs 12..15 are padding), W2 and
+ * W3 64x64, W4 8x64 (rows 2..7 zero); FP32 biases b1..b3 [64], b4 [8]; FP32 feature
+ * standardisation mean / istd [16]. */
+typedef struct {
+    uint16_t* W1;
+    uint16_t* W2;
+    uint16_t* W3;
+    uint16_t* W4;
+    float* b1;
+    float* b2;
+    float* b3;
+    float* b4;
+    float* mean;
+    float* istd;
+} ht_bracket_model;
+
+/* Number of FP32 parameters in the packed layout of ht_bracket_grad / ht_bracket_adam:
+ * W1 [64x16] W2 [64x64] W3 [64x64] W4 [8x64] b1 b2 b3 [64] b4 [8]. */
+#define HT_BRACKET_NPARAMS 9928
+
+/* Features [npeaks x 16] FP32 of the batch on the bound tile (ht_fields_pack first):
+ * Rf/alatt, sqrt(ir2min), delta_s at the peak (d_peak_delta, nullable), fcrit, ZZon,
+ * delta at the peak cell, mean delta on shells 2..5, rad[m0_init], Rf/alatt + 2, zeros. */
+HT_API int ht_bracket_features(ht_ctx* ctx, const ht_peak_batch* batch,
+                               const float* d_peak_delta, double alatt, float* d_feat,
+                               void* stream);
+
+/* Inference: d_pred [n x 2] FP32 (low, high quantile of the stop radius, lattice units)
+ * from d_feat [n x 16].  Tensor cores (mma.sync BF16, FP32 accumulation). */
+HT_API int ht_bracket_predict(ht_ctx* ctx, const ht_bracket_model* model, const float* d_feat,
+                              int64_t n, float* d_pred, void* stream);
+
+/* Training: pinball-loss gradient (quantiles 0.1 and 0.9 of d_target) over n rows,
+ * written to d_grads [HT_BRACKET_NPARAMS] in the packed layout; the mean loss to *d_loss. */
+HT_API int ht_bracket_grad(ht_ctx* ctx, const ht_bracket_model* model, const float* d_feat,
+                           const float* d_target, int64_t n, float* d_grads, float* d_loss,
+                           void* stream);
+
+/* One Adam step (beta 0.9 / 0.999, eps 1e-8) on packed FP32 master parameters, then the
+ * BF16 weights and FP32 biases of `model` are rewritten from them. */
+HT_API int ht_bracket_adam(ht_ctx* ctx, float* d_params, const float* d_grads, float* d_m,
+                           float* d_v, int32_t step, float lr, const ht_bracket_model* model,
+                           void* stream);
 
 /* Launch statistics of the last ht_shell_analyse on this context: kernels launched and
  * the total number of shells walked (for the roofline's algorithmic bytes). */
