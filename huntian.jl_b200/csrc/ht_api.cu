@@ -216,10 +216,11 @@ static double host_interp(const ht_ctx* c, double x, double y, double z) {
 static void free_ctx(ht_ctx* c) {
     if (c->fft_n) cufftDestroy(c->fft_plan);
     if (c->tile_n) cufftDestroy(c->tile_plan);
+    if (c->tp_n) { cufftDestroy(c->tp_plan_n); cufftDestroy(c->tp_plan_m); }
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
-                    c->d_mlp_ws, c->d_queue,
+                    c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_queue,
                     c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -443,6 +444,10 @@ extern "C" int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value) {
             if (value != 0 && (value < 2 || value > 1024))
                 return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: planes per CTA must be 0 or 2..1024");
             ctx->tune_pf_kz = (int)value;
+            return HT_OK;
+        case HT_TUNE_FFT_PATH:
+            if (value < 0 || value > 2) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: FFT path must be 0, 1 or 2");
+            ctx->tune_fft_path = (int)value;
             return HT_OK;
         case HT_TUNE_WALK_BPSM:
             if (value < 0 || value > 32) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: blocks per SM must be 0..32");

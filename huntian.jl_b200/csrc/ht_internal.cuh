@@ -44,6 +44,7 @@ struct ht_ctx {
     int tune_block_bits = 17;      // LEARNED order: spatial block of 2^bits cells
     int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)
     int tune_walk_bpsm = 0;        // walk: blocks per SM (0: occupancy maximum)
+    int tune_fft_path = 0;         // tile smoothing: 0 auto, 1 3-D plan, 2 transposed 1-D
 
     // collapse table + SPH table
     std::vector<float> h_ct;
@@ -71,6 +72,13 @@ struct ht_ctx {
     int fft_n = 0;
     cufftHandle tile_plan = 0;     // out-of-place C2R plan, unpadded output, tile_n^3
     int tile_n = 0;
+    void* d_cwork2 = nullptr;      // second complex buffer of the transposed path
+    size_t cwork2_bytes = 0;
+    cufftHandle tp_plan_n = 0;     // transposed path: 1-D C2C of length tp_n, batched
+    cufftHandle tp_plan_m = 0;     // and of length tp_n / 2
+    int tp_n = 0;
+    void* d_tw = nullptr;          // e^{2 pi i k / n}, k < n / 2
+    size_t tw_bytes = 0;
     void* d_order_ws = nullptr;    // BATCHED peak-order keys, indices and sort temp
     size_t order_ws_bytes = 0;
     void* d_mlp_ws = nullptr;      // bracket training activations

@@ -268,11 +268,11 @@ class HaloFinder:
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
 
     def tune(self, block_bits: Optional[int] = None, pf_kz: Optional[int] = None,
-             walk_bpsm: Optional[int] = None) -> None:
-        """Set result-neutral launch parameters (ht_ctx_tune)."""
+             walk_bpsm: Optional[int] = None, fft_path: Optional[int] = None) -> None:
+        """Set launch parameters (ht_ctx_tune); all but fft_path are result-neutral."""
         L = _lib.load()
         for key, v in ((_lib.HT_TUNE_BLOCK_BITS, block_bits), (_lib.HT_TUNE_PF_KZ, pf_kz),
-                       (_lib.HT_TUNE_WALK_BPSM, walk_bpsm)):
+                       (_lib.HT_TUNE_WALK_BPSM, walk_bpsm), (_lib.HT_TUNE_FFT_PATH, fft_path)):
             if v is not None:
                 check(L.ht_ctx_tune(self._h, key, int(v)))
 

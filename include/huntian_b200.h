@@ -140,8 +140,10 @@ HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, i
  * (ext/CUDAExt.jl:2951-2989): d_delta_k is the rfft of the n^3 tile itself (the tile is
  * treated as periodic with side boxsize = n * alatt), d_out (n^3 Float32 column-major)
  * receives irfft(W . delta_k) normalised by 1/n^3.  The window (W/n^3, FP64, rounded to
- * FP32 once) goes into a context buffer and one out-of-place cuFFT C2R writes the
- * unpadded tile directly (plan cached per n). */
+ * FP32 once) is applied on the way into a context buffer; the inverse transform is one
+ * out-of-place cuFFT C2R plan for power-of-two sides, and for other even sides three
+ * batched 1-D cuFFT transforms along axes made contiguous by transposes (cuFFT's 3-D plan
+ * is 3x slower there).  Plans cached per n; HT_TUNE_FFT_PATH overrides the choice. */
 HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
                           double boxsize, double Rf, int wsmooth, void* stream);
 
@@ -259,10 +261,15 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
  *                       2^value cells (Morton prefix) and ordered by descending predicted
  *                       cost inside a block (default 17);
  *   HT_TUNE_PF_KZ       peak scan: k-planes per CTA (0 = chosen from the grid size);
- *   HT_TUNE_WALK_BPSM   shell walk: resident blocks per SM (0 = the occupancy maximum). */
+ *   HT_TUNE_WALK_BPSM   shell walk: resident blocks per SM (0 = the occupancy maximum);
+ *   HT_TUNE_FFT_PATH    ht_smooth_tile's inverse FFT: 0 = by tile side (one 3-D cuFFT plan
+ *                       for powers of two, otherwise transposes + batched 1-D transforms),
+ *                       1 = 3-D plan, 2 = transposed 1-D (even sides).  The two differ by FP32
+ *                       round-off, so keep one choice per run for reproducible peaks. */
 #define HT_TUNE_BLOCK_BITS 1
 #define HT_TUNE_PF_KZ 2
 #define HT_TUNE_WALK_BPSM 3
+#define HT_TUNE_FFT_PATH 4
 HT_API int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value);
 
 /* ------------------------------------------------------ learned walk bracket ---- */

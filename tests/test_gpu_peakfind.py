@@ -171,11 +171,22 @@ def test_smooth_box_wrapped_matches_torch(ht, finder):
     assert torch.allclose(got, ref, rtol=1e-5, atol=1e-6 * float(ref.abs().max()))
 
 
-@pytest.mark.parametrize("n,wsmooth", [(36, 1), (40, 0), (30, 3)])
-def test_smooth_tile_matches_fp64(ht, finder, n, wsmooth):
-    """ht_smooth_tile (window with 1/n^3 folded in + out-of-place C2R into the unpadded
-    tile) vs numpy FP64 irfftn of the FP64-windowed rfft: the tile smoothing of
-    peak_find_tile_gpu (ext/CUDAExt.jl:2951-2989), boxsize = n * alatt."""
+@pytest.mark.parametrize("n,wsmooth,path", [(36, 1, 0), (40, 0, 0), (30, 3, 0), (32, 1, 0),
+                                            (36, 1, 1), (32, 1, 2), (44, 0, 2)])
+def test_smooth_tile_matches_fp64(ht, finder, n, wsmooth, path):
+    """ht_smooth_tile vs numpy FP64 irfftn of the FP64-windowed rfft: the tile smoothing of
+    peak_find_tile_gpu (ext/CUDAExt.jl:2951-2989), boxsize = n * alatt.  path 0 picks by
+    size (3-D cuFFT plan for powers of two, transposes + batched 1-D transforms for other
+    even sides); 1 and 2 force one of them."""
+    import torch
+    finder.tune(fft_path=path)
+    try:
+        _check_smooth_tile(finder, n, wsmooth)
+    finally:
+        finder.tune(fft_path=0)
+
+
+def _check_smooth_tile(finder, n, wsmooth):
     import torch
     alatt, Rf = 1.9, 5.0
     box = n * alatt
