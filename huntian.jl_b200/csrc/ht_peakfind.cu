@@ -117,11 +117,13 @@ constexpr int kBoxX = 40;                  // plane box width in floats (160 B)
 constexpr int kRowsPT = 4;                 // rows of j per thread
 constexpr int kTYB = kTY * kRowsPT;        // 32 rows of j per CTA
 constexpr int kBoxY = kTYB + 2;            // 34 rows: j - 1 .. j + 32
-constexpr int kStages = 8;                 // planes in flight per CTA
-constexpr int kPlaneBytes = kBoxX * kBoxY * 4;
-constexpr int kSlotFloats = 1376;          // 5504 B per slot: 128-byte aligned slots
+constexpr int kPPS = 2;                    // k-planes per TMA stage (box depth)
+constexpr int kStages = 4;                 // stages in flight per CTA (8 planes)
+constexpr int kPlaneFloats = kBoxX * kBoxY;                // 1360
+constexpr int kPlaneBytes = kPlaneFloats * 4 * kPPS;       // bytes of one stage's copy
+constexpr int kSlotFloats = 2720;          // 10880 B per stage: 128-byte aligned slots
 constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier wait: 2 s
-static_assert(kBoxX * kBoxY <= kSlotFloats && (kSlotFloats * 4) % 128 == 0, "slot size");
+static_assert(kPlaneFloats * kPPS <= kSlotFloats && (kSlotFloats * 4) % 128 == 0, "slot size");
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -161,9 +163,10 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parit
 }
 
 // One CTA: 32 (i) x 32 (j) cells over kz planes; thread (tx, ty) owns column i = ib + tx
-// and rows j = jb + 4 ty .. jb + 4 ty + 3.  Per plane it reads 6 rows x 3 columns of the
-// staged box and forms the 3 x 3 maxima of its 4 cells separably (vertical 3-maxima
-// sharing the middle pairs, then across the 3 columns).
+// and rows j = jb + 4 ty .. jb + 4 ty + 3.  Planes arrive two per TMA copy (a 40 x 34 x 2
+// box); per plane each thread reads 6 rows x 3 columns of the staged box and forms the
+// 3 x 3 maxima of its 4 cells separably (vertical 3-maxima sharing the middle pairs, then
+// across the 3 columns).  A stage is released once both of its planes are folded.
 __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     const __grid_constant__ CUtensorMap tm, const int8_t* __restrict__ mask,
     PfGeom g, float fcrit, int kz, uint32_t* __restrict__ bits, int32_t* __restrict__ status) {
@@ -181,7 +184,12 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     const int c0 = ib - 1 - x0 + tx;             // column of i - 1 inside the box
     const int r0 = kRowsPT * ty;                 // box row of j0 - 1
     const int nplanes = kend - kb + 2;           // planes kb - 1 .. kend
+    const int nstages = (nplanes + kPPS - 1) / kPPS;
     const long long n = g.n, nn = n * n;
+    // rows of this thread inside the inner range, and the bitmap word of (k = kb, j0)
+    const int nrows = max(0, min(kRowsPT, hi - j0));
+    long long word = ((long long)(kb - g.nbuff) * g.inner + (j0 - g.nbuff)) * g.wpr + blockIdx.x;
+    const long long word_step_k = (long long)g.inner * g.wpr;
 
     if (tid == 0) {
         for (int s = 0; s < kStages; ++s) {
@@ -191,14 +199,14 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
-    int issued = 0;
+    int issued = 0;   // stages issued (thread 0 only)
     if (tid == 0) {
-        for (; issued < kStages && issued < nplanes; ++issued)
-            tma_plane(ring[issued], &tm, x0, jb - 1, kb - 1 + issued, &full[issued]);
+        for (; issued < kStages && issued < nstages; ++issued)
+            tma_plane(ring[issued], &tm, x0, jb - 1, kb - 1 + kPPS * issued, &full[issued]);
     }
-    // 3x3 maxima of the thread's 4 cells in plane q, and their centre values
-    auto fold = [&](int q, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
-        const float* pl = ring[q % kStages] + r0 * kBoxX + c0;
+    // 3x3 maxima of the thread's 4 cells in plane p, and their centre values
+    auto fold = [&](int p, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
+        const float* pl = ring[(p / kPPS) % kStages] + (p % kPPS) * kPlaneFloats + r0 * kBoxX + c0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             float r[kRowsPT + 2];
@@ -219,54 +227,77 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
             }
         }
     };
-    // Consume plane q: wait for it, fold it, release its slot to plane q + kStages.
-    // Returns false (uniformly across the CTA) when a wait timed out.
-    int q_now = 0;
-    auto consume = [&](int q, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
-        q_now = q;
-        const bool ok = bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1));
-        fold(q, m, ctr);
+    int s_now = 0;
+    // wait for stage s; false (uniformly) when the wait timed out
+    auto wait_stage = [&](int s) {
+        s_now = s;
+        const bool ok = bar_wait(&full[s % kStages], (unsigned)((s / kStages) & 1));
+        return ok;
+    };
+    // all warps are done with stage s: hand its slot to stage s + kStages
+    auto release_stage = [&](bool ok) {
         if (__syncthreads_or(!ok)) return false;
-        if (tid == 0 && issued < nplanes) {
+        if (tid == 0 && issued < nstages) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            tma_plane(ring[issued % kStages], &tm, x0, jb - 1, kb - 1 + issued,
+            tma_plane(ring[issued % kStages], &tm, x0, jb - 1, kb - 1 + kPPS * issued,
                       &full[issued % kStages]);
             ++issued;
         }
         return true;
     };
-
     float mprev[kRowsPT], mcur[kRowsPT], mnext[kRowsPT];
-    float fprev[kRowsPT], ff[kRowsPT], fnext[kRowsPT];
-    bool ok = consume(0, mprev, fprev) && consume(1, mcur, ff);
-    for (int k = kb; ok && k < kend; ++k) {
-        ok = consume(k - kb + 2, mnext, fnext);
-        if (!ok) break;
+    float ff[kRowsPT], fnext[kRowsPT];
+    // the peak test of plane k (centre values ff, maxima of planes k-1, k, k+1)
+    auto test_plane = [&](int k) {
+        unsigned w[kRowsPT];
 #pragma unroll
         for (int rr = 0; rr < kRowsPT; ++rr) {
-            const int j = j0 + rr;
-            bool peak = false;
-            if (icol && j < hi) {
-                // ff < fcrit skips; any neighbour > ff rejects (ties pass); mask == 1
-                // skips.  fmaxf ignores NaN neighbours, matching `ff < NaN == false`.
-                const float m27 = fmaxf(fmaxf(mprev[rr], mcur[rr]), mnext[rr]);
-                peak = !(ff[rr] < fcrit) && !(ff[rr] < m27);
-                if (peak) peak = __ldg(mask + (long long)i + n * j + nn * k) != 1;
-            }
-            const unsigned w = __ballot_sync(0xffffffffu, peak);
-            if (tx == 0 && j < hi) {
-                const long long row = (long long)(k - g.nbuff) * g.inner + (j - g.nbuff);
-                bits[row * g.wpr + blockIdx.x] = w;
-            }
+            // ff < fcrit skips; any neighbour > ff rejects (ties pass); mask == 1 skips.
+            // fmaxf ignores NaN neighbours, matching `ff < NaN == false`.
+            const float m27 = fmaxf(fmaxf(mprev[rr], mcur[rr]), mnext[rr]);
+            bool peak = icol && rr < nrows && !(ff[rr] < fcrit) && !(ff[rr] < m27);
+            if (peak) peak = __ldg(mask + (long long)i + n * (j0 + rr) + nn * k) != 1;
+            w[rr] = __ballot_sync(0xffffffffu, peak);
+        }
+        // lane rr stores row rr's word
+        if (tx < nrows) {
+            unsigned v = w[0];
+#pragma unroll
+            for (int rr = 1; rr < kRowsPT; ++rr) v = tx == rr ? w[rr] : v;
+            bits[word + (long long)tx * g.wpr] = v;
+        }
+        word += word_step_k;
+#pragma unroll
+        for (int rr = 0; rr < kRowsPT; ++rr) {
             mprev[rr] = mcur[rr];
             mcur[rr] = mnext[rr];
             ff[rr] = fnext[rr];
         }
+    };
+
+    // stage 0 holds planes kb - 1 and kb
+    bool ok = wait_stage(0);
+    fold(0, mprev, ff);
+    fold(1, mcur, ff);
+    ok = release_stage(ok);
+    // each later stage s holds planes 2s, 2s + 1 (relative), i.e. k + 1 for k = kb + 2s - 2
+    for (int s = 1; ok && s < nstages; ++s) {
+        ok = wait_stage(s);
+        const int k = kb + kPPS * s - 2;      // the plane whose test needs plane 2s
+        if (k < kend) {
+            fold(kPPS * s, mnext, fnext);
+            test_plane(k);
+        }
+        if (k + 1 < kend) {
+            fold(kPPS * s + 1, mnext, fnext);
+            test_plane(k + 1);
+        }
+        ok = release_stage(ok);
     }
     if (!ok && tid == 0) {
         // record the timeout, then wait (bounded) for the copies still in flight
         atomicExch(status, 1);
-        for (int q = q_now; q < issued; ++q)
+        for (int q = s_now; q < issued; ++q)
             bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1));
     }
 }
@@ -414,7 +445,7 @@ bool pf_tensor_map(CUtensorMap* tm, const float* d, int n) {
     if (!enc) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)n};
     const cuuint64_t strides[2] = {(cuuint64_t)n * 4, (cuuint64_t)n * n * 4};
-    const cuuint32_t box[3] = {kBoxX, kBoxY, 1};
+    const cuuint32_t box[3] = {kBoxX, kBoxY, kPPS};
     const cuuint32_t estr[3] = {1, 1, 1};
     return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void*)d, dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -118,6 +118,7 @@ extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void*
 //   F2  1-D C2C along ky, in place on B
 //   T3  transpose B (z, kx, y) -> C (z, y, k) with the half-length real-inverse packing
 //       C[k] = (X[k] + conj X[m-k]) + i w^k (X[k] - conj X[m-k]),  m = n/2, w = e^{2 pi i/n}
+//       (outputs k and m - k come from the same two rows, so each row is read once)
 //   F3  1-D C2C of length m along k, batch n^2, out of place into the output: its complex
 //       result c[j] = x[2j] + i x[2j+1] is the real row itself.
 // Six HBM passes instead of the 3-D plan's slow decomposition; results agree with it to
@@ -167,33 +168,42 @@ __global__ void __launch_bounds__(256) t2_kernel(const float2* __restrict__ A,
     }
 }
 
-// C[(z N + y) m + k] from X[k] = B[(z NK + k) N + y] and X[m - k], k < m = N/2
+// C[(z N + y) m + k] from X[k] = B[(z NK + k) N + y] and X[m - k], k < m = N/2.  Outputs k
+// and m - k need the same two rows (X[k], X[m - k]), so a block loads a tile of "low" k in
+// [k0, k0 + 32) (k <= m/2) and its mirror tile once and writes both outputs: B is read once.
 __global__ void __launch_bounds__(256) t3_pack_kernel(const float2* __restrict__ B,
                                                       float2* __restrict__ C, int N, int NK,
                                                       const float2* __restrict__ tw) {
     __shared__ float2 ta[32][33];
     __shared__ float2 tb[32][33];
-    const int m = N / 2;
+    const int m = N / 2, half = m / 2;
     const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32, z = blockIdx.z;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int k = k0 + r, y = y0 + tx;
-        if (k < m && y < N) {
+        if (k <= half && y < N) {
             ta[r][tx] = __ldg(B + ((long long)z * NK + k) * N + y);
             tb[r][tx] = __ldg(B + ((long long)z * NK + (m - k)) * N + y);
         }
     }
     __syncthreads();
+    // packed value for output kk from a = X[kk], bb = X[m - kk]
+    auto pack = [&](float2 a, float2 bb, int kk) {
+        const float2 b = make_float2(bb.x, -bb.y);          // conj X[m - kk]
+        const float2 e = make_float2(a.x + b.x, a.y + b.y);
+        const float2 d = make_float2(a.x - b.x, a.y - b.y);
+        const float2 w = __ldg(tw + kk);
+        const float2 o = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
+        return make_float2(e.x - o.y, e.y + o.x);
+    };
     for (int r = ty; r < 32; r += 8) {
         const int k = k0 + tx, y = y0 + r;
-        if (k < m && y < N) {
-            const float2 a = ta[tx][r], bb = tb[tx][r];
-            const float2 b = make_float2(bb.x, -bb.y);          // conj X[m - k]
-            const float2 e = make_float2(a.x + b.x, a.y + b.y);
-            const float2 d = make_float2(a.x - b.x, a.y - b.y);
-            const float2 w = __ldg(tw + k);
-            const float2 o = make_float2(d.x * w.x - d.y * w.y, d.x * w.y + d.y * w.x);
-            C[((long long)z * N + y) * m + k] = make_float2(e.x - o.y, e.y + o.x);
+        if (k <= half && y < N) {
+            const float2 xa = ta[tx][r], xb = tb[tx][r];
+            float2* row = C + ((long long)z * N + y) * m;
+            row[k] = pack(xa, xb, k);                       // k < m always (k <= m/2)
+            const int kh = m - k;
+            if (kh != k && kh < m) row[kh] = pack(xb, xa, kh);
         }
     }
 }
@@ -269,8 +279,8 @@ static int smooth_tile_transposed(ht_ctx* ctx, const void* d_delta_k, float* d_o
     r = cufftExecC2C(ctx->tp_plan_n, (cufftComplex*)B, (cufftComplex*)B, CUFFT_INVERSE);
     if (r != CUFFT_SUCCESS) return ht_fail(HT_ERR_CUDA, "cufftExecC2C (y) failed with code " + std::to_string((int)r));
     const int m = n / 2;
-    t3_pack_kernel<<<dim3((unsigned)((m + 31) / 32), (unsigned)((n + 31) / 32), (unsigned)n), blk,
-                     0, st>>>(B, A, n, (int)nk, (const float2*)ctx->d_tw);
+    t3_pack_kernel<<<dim3((unsigned)((m / 2 + 1 + 31) / 32), (unsigned)((n + 31) / 32),
+                          (unsigned)n), blk, 0, st>>>(B, A, n, (int)nk, (const float2*)ctx->d_tw);
     HT_CUDA_TRY(cudaGetLastError(), "t3_pack_kernel launch");
     r = cufftExecC2C(ctx->tp_plan_m, (cufftComplex*)A, (cufftComplex*)d_out, CUFFT_INVERSE);
     if (r != CUFFT_SUCCESS) return ht_fail(HT_ERR_CUDA, "cufftExecC2C (x) failed with code " + std::to_string((int)r));
