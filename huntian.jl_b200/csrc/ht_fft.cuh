@@ -1,0 +1,180 @@
+// Warp-level inverse complex FFT of one column of L = 32 T points held in shared memory,
+// for the fused smoothing passes (ht_smooth.cu).  Convention: y[k] = sum_t x[t] e^{+2 pi i
+// t k / L} (unnormalised inverse).
+//
+// Four-step with L = 32 x T (Bailey 1990): lane l (0..31) owns x[l + 32 t], t = 0..T-1.
+//   1. each lane: T-point DFT over t in registers (mixed radix 2/3/4, composed),
+//   2. twiddle by e^{2 pi i l k2 / L},
+//   3. for every k2: 32-point DFT across the lanes with xor shuffles (radix-2,
+//      decimation in frequency: lane l ends with index k1 = bitrev5(l)),
+//   4. y[k2 + T k1] goes back to the column.
+// Small-DFT twiddles come from __constant__ tables of e^{2 pi i j / N} computed on the host
+// in FP64 (ht_fft_init); the lane-dependent step-2 twiddles from a per-L global table.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace htfft {
+
+struct C2 {
+    float x, y;
+};
+
+__device__ __forceinline__ C2 add(C2 a, C2 b) { return {a.x + b.x, a.y + b.y}; }
+__device__ __forceinline__ C2 sub(C2 a, C2 b) { return {a.x - b.x, a.y - b.y}; }
+__device__ __forceinline__ C2 mul(C2 a, C2 b) {
+    return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+__device__ __forceinline__ C2 muli(C2 a) { return {-a.y, a.x}; }   // i * a
+__device__ __forceinline__ C2 scale(C2 a, float s) { return {a.x * s, a.y * s}; }
+
+// e^{2 pi i j / N} for the small composite sizes used in registers (N = 9, 18, 36).
+extern __constant__ float2 c_w9[9];
+extern __constant__ float2 c_w18[18];
+extern __constant__ float2 c_w36[36];
+
+template <int N>
+__device__ __forceinline__ C2 wsmall(int j);   // e^{2 pi i j / N}, j in [0, N)
+template <>
+__device__ __forceinline__ C2 wsmall<9>(int j) { const float2 w = c_w9[j]; return {w.x, w.y}; }
+template <>
+__device__ __forceinline__ C2 wsmall<18>(int j) { const float2 w = c_w18[j]; return {w.x, w.y}; }
+template <>
+__device__ __forceinline__ C2 wsmall<36>(int j) { const float2 w = c_w36[j]; return {w.x, w.y}; }
+
+// In-register inverse DFT of N points; v[] in natural order on input and output.
+template <int N>
+struct Dft;
+
+template <>
+struct Dft<2> {
+    __device__ __forceinline__ static void run(C2 (&v)[2]) {
+        const C2 a = v[0], b = v[1];
+        v[0] = add(a, b);
+        v[1] = sub(a, b);
+    }
+};
+
+template <>
+struct Dft<3> {
+    __device__ __forceinline__ static void run(C2 (&v)[3]) {
+        const float h = 0.8660254037844386f;   // sqrt(3) / 2
+        const C2 a = v[0], s = add(v[1], v[2]), d = sub(v[1], v[2]);
+        const C2 m = {a.x - 0.5f * s.x, a.y - 0.5f * s.y};
+        const C2 id = scale(muli(d), h);
+        v[0] = add(a, s);
+        v[1] = add(m, id);
+        v[2] = sub(m, id);
+    }
+};
+
+template <>
+struct Dft<4> {
+    __device__ __forceinline__ static void run(C2 (&v)[4]) {
+        const C2 t0 = add(v[0], v[2]), t1 = sub(v[0], v[2]);
+        const C2 t2 = add(v[1], v[3]), t3 = muli(sub(v[1], v[3]));
+        v[0] = add(t0, t2);
+        v[2] = sub(t0, t2);
+        v[1] = add(t1, t3);
+        v[3] = sub(t1, t3);
+    }
+};
+
+// N = R1 R2: x[t1 + R1 t2] -> y[k2 + R2 k1] = sum_t1 w_R1^{t1 k1} w_N^{t1 k2}
+//                                               sum_t2 x[t1 + R1 t2] w_R2^{t2 k2}
+template <int R1, int R2>
+struct DftComposite {
+    static constexpr int N = R1 * R2;
+    __device__ __forceinline__ static void run(C2 (&v)[N]) {
+        C2 u[N];
+#pragma unroll
+        for (int t1 = 0; t1 < R1; ++t1) {
+            C2 a[R2];
+#pragma unroll
+            for (int t2 = 0; t2 < R2; ++t2) a[t2] = v[t1 + R1 * t2];
+            Dft<R2>::run(a);
+#pragma unroll
+            for (int k2 = 0; k2 < R2; ++k2)
+                u[t1 + R1 * k2] = (t1 * k2) % N == 0 ? a[k2] : mul(a[k2], wsmall<N>((t1 * k2) % N));
+        }
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+            C2 b[R1];
+#pragma unroll
+            for (int t1 = 0; t1 < R1; ++t1) b[t1] = u[t1 + R1 * k2];
+            Dft<R1>::run(b);
+#pragma unroll
+            for (int k1 = 0; k1 < R1; ++k1) v[k2 + R2 * k1] = b[k1];
+        }
+    }
+};
+
+template <>
+struct Dft<9> {
+    __device__ __forceinline__ static void run(C2 (&v)[9]) { DftComposite<3, 3>::run(v); }
+};
+template <>
+struct Dft<18> {
+    __device__ __forceinline__ static void run(C2 (&v)[18]) { DftComposite<2, 9>::run(v); }
+};
+template <>
+struct Dft<36> {
+    __device__ __forceinline__ static void run(C2 (&v)[36]) { DftComposite<4, 9>::run(v); }
+};
+
+__device__ __forceinline__ int bitrev5(int l) { return __brev((unsigned)l) >> 27; }
+
+// Inverse FFT of the column col[0 .. 32 T) (shared memory, float2), in place.
+// twL[j] = e^{2 pi i j / (32 T)}, j < 32 T (global, cached).  w32[s] for the cross-lane
+// stages (precomputed by the caller per lane): w32[s] = e^{2 pi i (lane mod 2^s) / 2^{s+1}}.
+template <int T>
+__device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict__ twL, int lane,
+                                          const C2 (&w32)[5]) {
+    constexpr int L = 32 * T;
+    C2 v[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const float2 e = col[lane + 32 * t];
+        v[t] = {e.x, e.y};
+    }
+    Dft<T>::run(v);
+#pragma unroll
+    for (int k2 = 1; k2 < T; ++k2) {
+        const float2 w = __ldg(twL + (lane * k2) % L);
+        v[k2] = mul(v[k2], {w.x, w.y});
+    }
+    // 32-point DFT across lanes, decimation in frequency: spans 16, 8, 4, 2, 1
+#pragma unroll
+    for (int st = 4; st >= 0; --st) {
+        const int s = 1 << st;
+        const bool upper = (lane & s) != 0;
+#pragma unroll
+        for (int k2 = 0; k2 < T; ++k2) {
+            C2 a = v[k2];
+            C2 b = {__shfl_xor_sync(0xffffffffu, a.x, s), __shfl_xor_sync(0xffffffffu, a.y, s)};
+            // lower lane: a + b; upper lane: (b - a) * w_{2s}^{lane mod s}
+            const C2 lo = add(a, b);
+            const C2 hi = mul(sub(b, a), w32[st]);
+            v[k2] = upper ? hi : lo;
+        }
+    }
+    __syncwarp();
+    const int k1 = bitrev5(lane);
+#pragma unroll
+    for (int k2 = 0; k2 < T; ++k2) col[k2 + T * k1] = make_float2(v[k2].x, v[k2].y);
+    __syncwarp();
+}
+
+// Per-lane cross-lane twiddles for warp_ifft: w32[st] = e^{2 pi i (lane mod 2^st) / 2^(st+1)}
+__device__ __forceinline__ void lane_twiddles(int lane, const float2* __restrict__ tw32,
+                                              C2 (&w32)[5]) {
+#pragma unroll
+    for (int st = 0; st < 5; ++st) {
+        const int s = 1 << st;
+        // e^{2 pi i j / (2s)} = e^{2 pi i j (16 / s) / 32}, j = lane mod s
+        const float2 w = __ldg(tw32 + ((lane & (s - 1)) * (16 / s)));
+        w32[st] = {w.x, w.y};
+    }
+}
+
+}  // namespace htfft
