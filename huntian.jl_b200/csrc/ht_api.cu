@@ -220,7 +220,7 @@ static void free_ctx(ht_ctx* c) {
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
-                    c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_queue,
+                    c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_ftw, c->d_queue,
                     c->d_stats};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -446,7 +446,7 @@ extern "C" int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value) {
             ctx->tune_pf_kz = (int)value;
             return HT_OK;
         case HT_TUNE_FFT_PATH:
-            if (value < 0 || value > 2) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: FFT path must be 0, 1 or 2");
+            if (value < 0 || value > 3) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: FFT path must be 0..3");
             ctx->tune_fft_path = (int)value;
             return HT_OK;
         case HT_TUNE_WALK_BPSM:

@@ -9,7 +9,8 @@
 //      decimation in frequency: lane l ends with index k1 = bitrev5(l)),
 //   4. y[k2 + T k1] goes back to the column.
 // Small-DFT twiddles come from __constant__ tables of e^{2 pi i j / N} computed on the host
-// in FP64 (ht_fft_init); the lane-dependent step-2 twiddles from a per-L global table.
+// in FP64 (fused_tables in ht_smooth.cu); the lane-dependent step-2 twiddles from a per-L
+// global table.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -28,10 +29,11 @@ __device__ __forceinline__ C2 mul(C2 a, C2 b) {
 __device__ __forceinline__ C2 muli(C2 a) { return {-a.y, a.x}; }   // i * a
 __device__ __forceinline__ C2 scale(C2 a, float s) { return {a.x * s, a.y * s}; }
 
-// e^{2 pi i j / N} for the small composite sizes used in registers (N = 9, 18, 36).
-extern __constant__ float2 c_w9[9];
-extern __constant__ float2 c_w18[18];
-extern __constant__ float2 c_w36[36];
+// e^{2 pi i j / N} for the small composite sizes used in registers (N = 9, 18, 36); this
+// header belongs to one translation unit (ht_smooth.cu), which fills them at set-up.
+__constant__ float2 c_w9[9];
+__constant__ float2 c_w18[18];
+__constant__ float2 c_w36[36];
 
 template <int N>
 __device__ __forceinline__ C2 wsmall(int j);   // e^{2 pi i j / N}, j in [0, N)

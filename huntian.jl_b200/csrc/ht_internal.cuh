@@ -44,7 +44,8 @@ struct ht_ctx {
     int tune_block_bits = 17;      // LEARNED order: spatial block of 2^bits cells
     int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)
     int tune_walk_bpsm = 0;        // walk: blocks per SM (0: occupancy maximum)
-    int tune_fft_path = 0;         // tile smoothing: 0 auto, 1 3-D plan, 2 transposed 1-D
+    int tune_fft_path = 0;         // tile smoothing: 0 auto, 1 3-D plan, 2 transposed 1-D,
+                                   // 3 fused three-pass (n = 576, 1152)
 
     // collapse table + SPH table
     std::vector<float> h_ct;
@@ -79,6 +80,9 @@ struct ht_ctx {
     int tp_n = 0;
     void* d_tw = nullptr;          // e^{2 pi i k / n}, k < n / 2
     size_t tw_bytes = 0;
+    void* d_ftw = nullptr;         // fused-path twiddles for side fz_n
+    size_t ftw_bytes = 0;
+    int fz_n = 0;
     void* d_order_ws = nullptr;    // BATCHED peak-order keys, indices and sort temp
     size_t order_ws_bytes = 0;
     void* d_mlp_ws = nullptr;      // bracket training activations

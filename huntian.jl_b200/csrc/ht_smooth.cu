@@ -11,6 +11,7 @@
 #include <string>
 #include <vector>
 
+#include "ht_fft.cuh"
 #include "ht_internal.cuh"
 
 namespace {
@@ -288,6 +289,206 @@ static int smooth_tile_transposed(ht_ctx* ctx, const void* d_delta_k, float* d_o
     return HT_OK;
 }
 
+
+// --------------------------------------------- fused three-pass inverse FFT (n = 32 T) ----
+//
+// For tile sides n = 576 and 1152 the six passes of the transposed path can collapse into
+// three (ht_fft.cuh): each kernel loads 8 columns along the axis it transforms (64-byte
+// segments of 8 neighbours), runs one warp-level inverse FFT per column in shared memory,
+// and stores every column contiguously in the next pass's layout (the default at 576 only:
+// at 1152 the 64-byte reads keep it slower than the transposed path):
+//   Z  window (with 1/n^3) on load, FFT along kz:     (kz, ky, kx) -> A (ky, kx, z)
+//   Y  FFT along ky:                                   A (ky, kx, z) -> B (z, kx, y)
+//   X  half-length real packing, FFT of n/2 along kx:  B (z, kx, y) -> out (z, y, x)
+
+namespace {
+
+constexpr int kFftCols = 8;   // columns (warps) per CTA
+
+template <int T>
+__global__ void __launch_bounds__(256) fft_z_kernel(const float2* __restrict__ in,
+                                                    float2* __restrict__ A, int NK,
+                                                    const float* __restrict__ tab,
+                                                    const float2* __restrict__ twL,
+                                                    const float2* __restrict__ tw32) {
+    constexpr int N = 32 * T, S = N + 1;
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int kx0 = blockIdx.x * kFftCols, ky = blockIdx.y;
+    const int sy = ky <= N / 2 ? ky : ky - N;
+    for (int e = tid; e < kFftCols * N; e += blockDim.x) {
+        const int r = e / kFftCols, c = e % kFftCols;      // r = kz
+        const int kx = kx0 + c;
+        float2 v = make_float2(0.f, 0.f);
+        if (kx < NK) {
+            const int sz = r <= N / 2 ? r : r - N;
+            const float wv = __ldg(tab + (kx * kx + sy * sy + sz * sz));
+            v = __ldg(in + ((long long)r * N + ky) * NK + kx);
+            v.x *= wv;
+            v.y *= wv;
+        }
+        sm[c * S + r] = v;
+    }
+    __syncthreads();
+    const int kx = kx0 + w;
+    if (kx >= NK) return;
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    float2* col = sm + w * S;
+    htfft::warp_ifft<T>(col, twL, lane, w32);
+    float2* dst = A + ((long long)ky * NK + kx) * N;
+    for (int z = lane; z < N; z += 32) dst[z] = col[z];
+}
+
+template <int T>
+__global__ void __launch_bounds__(256) fft_y_kernel(const float2* __restrict__ A,
+                                                    float2* __restrict__ B, int NK,
+                                                    const float2* __restrict__ twL,
+                                                    const float2* __restrict__ tw32) {
+    constexpr int N = 32 * T, S = N + 1;
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int z0 = blockIdx.x * kFftCols, kx = blockIdx.y;
+    for (int e = tid; e < kFftCols * N; e += blockDim.x) {
+        const int r = e / kFftCols, c = e % kFftCols;      // r = ky
+        const int z = z0 + c;
+        sm[c * S + r] = z < N ? __ldg(A + ((long long)r * NK + kx) * N + z) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int z = z0 + w;
+    if (z >= N) return;
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    float2* col = sm + w * S;
+    htfft::warp_ifft<T>(col, twL, lane, w32);
+    float2* dst = B + ((long long)z * NK + kx) * N;
+    for (int y = lane; y < N; y += 32) dst[y] = col[y];
+}
+
+// TH = n / 64: the packed rows have m = n / 2 = 32 TH points
+template <int TH>
+__global__ void __launch_bounds__(256) fft_x_kernel(const float2* __restrict__ B,
+                                                    float2* __restrict__ out, int NK,
+                                                    const float2* __restrict__ twp,
+                                                    const float2* __restrict__ twM,
+                                                    const float2* __restrict__ tw32) {
+    constexpr int M = 32 * TH, N = 2 * M, S = M + 2;
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int y0 = blockIdx.x * kFftCols, z = blockIdx.y;
+    for (int e = tid; e < kFftCols * NK; e += blockDim.x) {
+        const int r = e / kFftCols, c = e % kFftCols;      // r = kx
+        const int y = y0 + c;
+        sm[c * S + r] = y < N ? __ldg(B + ((long long)z * NK + r) * N + y) : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const int y = y0 + w;
+    if (y >= N) return;
+    float2* col = sm + w * S;
+    // in-place packing: lane handles the pair (k, M - k) for k = lane, lane + 32, ... <= M/2
+    for (int k = lane; k <= M / 2; k += 32) {
+        const float2 xa = col[k], xb = col[M - k];
+        auto pack = [&](float2 a, float2 bb, int kk) {
+            const float2 b = make_float2(bb.x, -bb.y);
+            const float2 e = make_float2(a.x + b.x, a.y + b.y);
+            const float2 d = make_float2(a.x - b.x, a.y - b.y);
+            const float2 wv = __ldg(twp + kk);
+            const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
+            return make_float2(e.x - o.y, e.y + o.x);
+        };
+        const float2 zk = pack(xa, xb, k);
+        const int kh = M - k;
+        if (kh != k && kh < M) col[kh] = pack(xb, xa, kh);
+        col[k] = zk;
+    }
+    __syncwarp();
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    htfft::warp_ifft<TH>(col, twM, lane, w32);
+    float2* dst = out + ((long long)z * N + y) * M;
+    for (int j = lane; j < M; j += 32) dst[j] = col[j];
+}
+
+}  // namespace
+
+// Twiddle tables of the fused path for side n (FP64 on the host, stored as FP32).
+static int fused_tables(ht_ctx* ctx, int n) {
+    if (ctx->fz_n == n) return HT_OK;
+    std::vector<float2> t((size_t)n + n / 2 + 32);
+    auto w = [](double j, double N) {
+        const double ph = 2.0 * 3.14159265358979323846 * j / N;
+        return make_float2((float)cos(ph), (float)sin(ph));
+    };
+    for (int j = 0; j < n; ++j) t[j] = w(j, n);               // e^{2 pi i j / n}
+    for (int j = 0; j < n / 2; ++j) t[n + j] = w(j, n / 2);   // e^{2 pi i j / (n/2)}
+    for (int j = 0; j < 32; ++j) t[n + n / 2 + j] = w(j, 32);
+    int rc = ht_grow(&ctx->d_ftw, &ctx->ftw_bytes, t.size() * sizeof(float2), "FFT twiddles");
+    if (rc != HT_OK) return rc;
+    HT_CUDA_TRY(cudaMemcpy(ctx->d_ftw, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice),
+                "twiddle upload");
+    float2 c9[9], c18[18], c36[36];
+    for (int j = 0; j < 9; ++j) c9[j] = w(j, 9);
+    for (int j = 0; j < 18; ++j) c18[j] = w(j, 18);
+    for (int j = 0; j < 36; ++j) c36[j] = w(j, 36);
+    HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w9, c9, sizeof c9), "c_w9");
+    HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w18, c18, sizeof c18), "c_w18");
+    HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w36, c36, sizeof c36), "c_w36");
+    ctx->fz_n = n;
+    return HT_OK;
+}
+
+template <int T>
+static int launch_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, cudaStream_t st) {
+    constexpr int n = 32 * T;
+    const int nk = n / 2 + 1, m = n / 2;
+    const size_t smz = (size_t)kFftCols * (n + 1) * sizeof(float2);
+    const size_t smx = (size_t)kFftCols * (m + 2) * sizeof(float2);
+    const float2* tw = (const float2*)ctx->d_ftw;
+    const float2* twL = tw;              // n
+    const float2* twM = tw + n;          // n / 2
+    const float2* tw32 = tw + n + n / 2;
+    HT_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz), "fft_z smem");
+    HT_CUDA_TRY(cudaFuncSetAttribute(fft_y_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz), "fft_y smem");
+    HT_CUDA_TRY(cudaFuncSetAttribute(fft_x_kernel<T / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "fft_x smem");
+    float2* A = (float2*)ctx->d_cwork;
+    float2* B = (float2*)ctx->d_cwork2;
+    fft_z_kernel<T><<<dim3((unsigned)((nk + kFftCols - 1) / kFftCols), (unsigned)n), 256, smz, st>>>(
+        (const float2*)d_delta_k, A, nk, (const float*)ctx->d_win, twL, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "fft_z_kernel launch");
+    fft_y_kernel<T><<<dim3((unsigned)((n + kFftCols - 1) / kFftCols), (unsigned)nk), 256, smz, st>>>(
+        A, B, nk, twL, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "fft_y_kernel launch");
+    fft_x_kernel<T / 2><<<dim3((unsigned)((n + kFftCols - 1) / kFftCols), (unsigned)n), 256, smx, st>>>(
+        B, (float2*)d_out, nk, (const float2*)ctx->d_tw, twM, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "fft_x_kernel launch");
+    (void)m;
+    return HT_OK;
+}
+
+static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                             double boxsize, double Rf, int wsmooth, cudaStream_t st) {
+    const long long nk = n / 2 + 1;
+    const size_t cbytes = (size_t)nk * n * n * sizeof(float2);
+    int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
+    if (rc == HT_OK) rc = ht_grow(&ctx->d_cwork2, &ctx->cwork2_bytes, cbytes, "smoothing buffer 2");
+    if (rc == HT_OK) rc = transposed_plans(ctx, n);   // the pack twiddles e^{2 pi i k / n}
+    if (rc == HT_OK) rc = fused_tables(ctx, n);
+    if (rc != HT_OK) return rc;
+    const int h = n / 2;
+    const int nvals = 3 * h * h + 1;
+    rc = ht_grow(&ctx->d_win, &ctx->win_bytes, (size_t)nvals * sizeof(float), "window table");
+    if (rc != HT_OK) return rc;
+    const double dk = 2.0 * 3.14159265358979323846 / boxsize;
+    window_table_kernel<<<(nvals + 255) / 256, 256, 0, st>>>((float*)ctx->d_win, nvals, dk, Rf,
+                                                             wsmooth, 1.0 / ((double)n * n * n));
+    HT_CUDA_TRY(cudaGetLastError(), "window_table_kernel launch");
+    rc = n == 1152 ? launch_fused<36>(ctx, d_delta_k, d_out, st)
+                   : launch_fused<18>(ctx, d_delta_k, d_out, st);
+    if (rc != HT_OK) return rc;
+    ctx->last_kernels = 4;
+    return HT_OK;
+}
+
 // ------------------------------------------------------ window + inverse FFT (tile) ----
 
 extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
@@ -301,7 +502,15 @@ extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* 
     // path: the single 3-D plan for power-of-two sides (and odd ones), the transposed
     // 1-D pipeline otherwise; HT_TUNE_FFT_PATH overrides (1 = 3-D plan, 2 = transposed)
     const bool pow2 = (n & (n - 1)) == 0;
-    const int path = ctx->tune_fft_path ? ctx->tune_fft_path : (pow2 || (n & 1) ? 1 : 2);
+    // fused three-pass kernels: measured faster at 576 (1.84 vs 2.39 ms) but not at 1152
+    // (20.1 vs 16.3 ms: 8-column tiles read 64-byte pieces of HBM rows), so by default only
+    // there
+    const bool fused_ok = n == 576 || n == 1152;
+    const int path = ctx->tune_fft_path ? ctx->tune_fft_path
+                                        : (n == 576 ? 3 : (pow2 || (n & 1) ? 1 : 2));
+    if (path == 3 && fused_ok)
+        return smooth_tile_fused(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth,
+                                 (cudaStream_t)stream);
     if (path == 2 && (n & 1) == 0 && (long long)n * (n / 2 + 1) < 0x7fffffffLL)
         return smooth_tile_transposed(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth,
                                       (cudaStream_t)stream);

@@ -263,8 +263,9 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
  *   HT_TUNE_PF_KZ       peak scan: k-planes per CTA (0 = chosen from the grid size);
  *   HT_TUNE_WALK_BPSM   shell walk: resident blocks per SM (0 = the occupancy maximum);
  *   HT_TUNE_FFT_PATH    ht_smooth_tile's inverse FFT: 0 = by tile side (one 3-D cuFFT plan
- *                       for powers of two, otherwise transposes + batched 1-D transforms),
- *                       1 = 3-D plan, 2 = transposed 1-D (even sides).  The two differ by FP32
+ *                       for powers of two, the fused three-pass kernels at 576, otherwise
+ *                       transposes + batched 1-D transforms), 1 = 3-D plan, 2 = transposed
+ *                       1-D (even sides), 3 = fused (sides 576 and 1152).  They differ by FP32
  *                       round-off, so keep one choice per run for reproducible peaks. */
 #define HT_TUNE_BLOCK_BITS 1
 #define HT_TUNE_PF_KZ 2

@@ -209,3 +209,26 @@ def _check_smooth_tile(finder, n, wsmooth):
     assert got.shape == (n, n, n) and got.dtype == np.float32
     # FP32 FFT round-off: a few ulp of the field's range
     assert np.abs(got - ref).max() <= 2e-6 * scale * np.log2(n ** 3)
+
+
+@pytest.mark.parametrize("n", [576, 1152])
+def test_fused_fft_matches_transposed_path(ht, finder, n):
+    """The fused three-pass inverse FFT (warp-level FFTs in shared memory, sides 576 and
+    1152) against the transposed cuFFT path (itself checked against FP64 above): the same
+    transform up to FP32 round-off."""
+    import torch
+    rng = np.random.default_rng(n)
+    a = torch.as_tensor(rng.standard_normal((n, n, n)).astype(np.float32), device="cuda")
+    ak = torch.fft.rfftn(a, dim=(0, 1, 2)).contiguous()
+    del a
+    outs = []
+    try:
+        for path in (2, 3):
+            finder.tune(fft_path=path)
+            outs.append(finder.smooth_tile(ak, n, n * 1.46, 6.0, 1).cpu().numpy())
+    finally:
+        finder.tune(fft_path=0)
+    ref, got = outs
+    scale = np.abs(ref).max()
+    assert np.abs(got - ref).max() <= 2e-6 * scale * np.log2(n ** 3)
+    assert finder.device_status() == 0
