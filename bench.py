@@ -189,7 +189,9 @@ class Workload:
     def smooth(self, Rf):
         if getattr(self, "_ds", None) is None:
             self._ds = torch.empty((self.nt,) * 3, dtype=torch.float32, device=self.device)
-        return self.finder.smooth_tile(self.dk, self.nt, self.boxsize, Rf, 1, out=self._ds)
+        # only the planes the peak scan reads: nbuff - 1 .. nt - nbuff
+        return self.finder.smooth_tile(self.dk, self.nt, self.boxsize, Rf, 1, out=self._ds,
+                                       planes=(self.nbuff - 1, self.nt - self.nbuff + 1))
 
     def pf_loop(self, ev=None):
         """Per filter: window + C2R of the tile (ht_smooth_tile), then the peak scan."""

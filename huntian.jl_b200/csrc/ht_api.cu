@@ -216,7 +216,8 @@ static double host_interp(const ht_ctx* c, double x, double y, double z) {
 static void free_ctx(ht_ctx* c) {
     if (c->fft_n) cufftDestroy(c->fft_plan);
     if (c->tile_n) cufftDestroy(c->tile_plan);
-    if (c->tp_n) { cufftDestroy(c->tp_plan_n); cufftDestroy(c->tp_plan_m); }
+    if (c->tp_n) cufftDestroy(c->tp_plan_n);
+    if (c->tp_zc) { cufftDestroy(c->tp_plan_y); cufftDestroy(c->tp_plan_x); }
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,

@@ -75,9 +75,11 @@ struct ht_ctx {
     int tile_n = 0;
     void* d_cwork2 = nullptr;      // second complex buffer of the transposed path
     size_t cwork2_bytes = 0;
-    cufftHandle tp_plan_n = 0;     // transposed path: 1-D C2C of length tp_n, batched
-    cufftHandle tp_plan_m = 0;     // and of length tp_n / 2
+    cufftHandle tp_plan_n = 0;     // transposed path: 1-D C2C of length tp_n, all rows
     int tp_n = 0;
+    cufftHandle tp_plan_y = 0;     // length tp_zc_n along y for tp_zc planes
+    cufftHandle tp_plan_x = 0;     // length tp_zc_n / 2 along x for tp_zc planes
+    int tp_zc = 0, tp_zc_n = 0;
     void* d_tw = nullptr;          // e^{2 pi i k / n}, k < n / 2
     size_t tw_bytes = 0;
     void* d_ftw = nullptr;         // fused-path twiddles for side fz_n

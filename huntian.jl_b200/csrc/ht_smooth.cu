@@ -152,20 +152,21 @@ __global__ void __launch_bounds__(256) t1_window_kernel(const float2* __restrict
     }
 }
 
-// B[(z NK + kx) N + ky] = A[(ky NK + kx) N + z]
+// B[(z NK + kx) N + ky] = A[(ky NK + kx) N + z] for z in [zlo, zhi)
 __global__ void __launch_bounds__(256) t2_kernel(const float2* __restrict__ A,
-                                                 float2* __restrict__ B, int N, int NK) {
+                                                 float2* __restrict__ B, int N, int NK,
+                                                 int zlo, int zhi) {
     __shared__ float2 t[32][33];
-    const int z0 = blockIdx.x * 32, y0 = blockIdx.y * 32, kx = blockIdx.z;
+    const int z0 = zlo + blockIdx.x * 32, y0 = blockIdx.y * 32, kx = blockIdx.z;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int ky = y0 + r, z = z0 + tx;
-        if (ky < N && z < N) t[r][tx] = __ldg(A + ((long long)ky * NK + kx) * N + z);
+        if (ky < N && z < zhi) t[r][tx] = __ldg(A + ((long long)ky * NK + kx) * N + z);
     }
     __syncthreads();
     for (int r = ty; r < 32; r += 8) {
         const int z = z0 + r, ky = y0 + tx;
-        if (ky < N && z < N) B[((long long)z * NK + kx) * N + ky] = t[tx][r];
+        if (ky < N && z < zhi) B[((long long)z * NK + kx) * N + ky] = t[tx][r];
     }
 }
 
@@ -174,11 +175,11 @@ __global__ void __launch_bounds__(256) t2_kernel(const float2* __restrict__ A,
 // [k0, k0 + 32) (k <= m/2) and its mirror tile once and writes both outputs: B is read once.
 __global__ void __launch_bounds__(256) t3_pack_kernel(const float2* __restrict__ B,
                                                       float2* __restrict__ C, int N, int NK,
-                                                      const float2* __restrict__ tw) {
+                                                      const float2* __restrict__ tw, int zlo) {
     __shared__ float2 ta[32][33];
     __shared__ float2 tb[32][33];
     const int m = N / 2, half = m / 2;
-    const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32, z = blockIdx.z;
+    const int k0 = blockIdx.x * 32, y0 = blockIdx.y * 32, z = zlo + blockIdx.z;
     const int tx = threadIdx.x, ty = threadIdx.y;
     for (int r = ty; r < 32; r += 8) {
         const int k = k0 + r, y = y0 + tx;
@@ -212,11 +213,34 @@ __global__ void __launch_bounds__(256) t3_pack_kernel(const float2* __restrict__
 }  // namespace
 
 // Build (once per n) the 1-D plans and the twiddles of the transposed path.
+// F2 / F3 plans for zc planes (the peak scan needs only the inner planes of the tile)
+static int transposed_plane_plans(ht_ctx* ctx, int n, int zc) {
+    if (ctx->tp_zc_n == n && ctx->tp_zc == zc) return HT_OK;
+    if (ctx->tp_zc) {
+        cufftDestroy(ctx->tp_plan_y);
+        cufftDestroy(ctx->tp_plan_x);
+        ctx->tp_zc = 0;
+    }
+    const int nk = n / 2 + 1, m = n / 2;
+    int len[1] = {n}, lm[1] = {m};
+    cufftResult r = cufftPlanMany(&ctx->tp_plan_y, 1, len, len, 1, n, len, 1, n, CUFFT_C2C,
+                                  zc * nk);
+    if (r != CUFFT_SUCCESS)
+        return ht_fail(HT_ERR_CUDA, "cufftPlanMany(C2C, y planes) failed with code " + std::to_string((int)r));
+    r = cufftPlanMany(&ctx->tp_plan_x, 1, lm, lm, 1, m, lm, 1, m, CUFFT_C2C, zc * n);
+    if (r != CUFFT_SUCCESS) {
+        cufftDestroy(ctx->tp_plan_y);
+        return ht_fail(HT_ERR_CUDA, "cufftPlanMany(C2C, x planes) failed with code " + std::to_string((int)r));
+    }
+    ctx->tp_zc = zc;
+    ctx->tp_zc_n = n;
+    return HT_OK;
+}
+
 static int transposed_plans(ht_ctx* ctx, int n) {
     if (ctx->tp_n == n) return HT_OK;
     if (ctx->tp_n) {
         cufftDestroy(ctx->tp_plan_n);
-        cufftDestroy(ctx->tp_plan_m);
         ctx->tp_n = 0;
     }
     if (ht_fault_injected("alloc")) return ht_fail(HT_ERR_FAULT, "injected allocation fault: cuFFT plan");
@@ -226,12 +250,6 @@ static int transposed_plans(ht_ctx* ctx, int n) {
                                   n * nk);
     if (r != CUFFT_SUCCESS)
         return ht_fail(HT_ERR_CUDA, "cufftPlanMany(C2C, n) failed with code " + std::to_string((int)r));
-    int lm[1] = {m};
-    r = cufftPlanMany(&ctx->tp_plan_m, 1, lm, lm, 1, m, lm, 1, m, CUFFT_C2C, n * n);
-    if (r != CUFFT_SUCCESS) {
-        cufftDestroy(ctx->tp_plan_n);
-        return ht_fail(HT_ERR_CUDA, "cufftPlanMany(C2C, n/2) failed with code " + std::to_string((int)r));
-    }
     std::vector<float2> tw((size_t)m);
     for (int k = 0; k < m; ++k) {
         const double ph = 2.0 * 3.14159265358979323846 * (double)k / (double)n;
@@ -246,12 +264,14 @@ static int transposed_plans(ht_ctx* ctx, int n) {
 }
 
 static int smooth_tile_transposed(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
-                                  double boxsize, double Rf, int wsmooth, cudaStream_t st) {
+                                  double boxsize, double Rf, int wsmooth, int zlo, int zhi,
+                                  cudaStream_t st) {
     const long long nk = n / 2 + 1;
     const size_t cbytes = (size_t)nk * n * n * sizeof(float2);
     int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
     if (rc == HT_OK) rc = ht_grow(&ctx->d_cwork2, &ctx->cwork2_bytes, cbytes, "smoothing buffer 2");
     if (rc == HT_OK) rc = transposed_plans(ctx, n);
+    if (rc == HT_OK) rc = transposed_plane_plans(ctx, n, zhi - zlo);
     if (rc != HT_OK) return rc;
     // window table (W / n^3 per distinct integer |k|^2), shared with the other paths
     const int h = n / 2;
@@ -270,20 +290,26 @@ static int smooth_tile_transposed(ht_ctx* ctx, const void* d_delta_k, float* d_o
                                      (const float*)ctx->d_win);
     HT_CUDA_TRY(cudaGetLastError(), "t1_window_kernel launch");
     if (cufftSetStream(ctx->tp_plan_n, st) != CUFFT_SUCCESS ||
-        cufftSetStream(ctx->tp_plan_m, st) != CUFFT_SUCCESS)
+        cufftSetStream(ctx->tp_plan_y, st) != CUFFT_SUCCESS ||
+        cufftSetStream(ctx->tp_plan_x, st) != CUFFT_SUCCESS)
         return ht_fail(HT_ERR_CUDA, "cufftSetStream failed");
     cufftResult r = cufftExecC2C(ctx->tp_plan_n, (cufftComplex*)A, (cufftComplex*)A, CUFFT_INVERSE);
     if (r != CUFFT_SUCCESS) return ht_fail(HT_ERR_CUDA, "cufftExecC2C (z) failed with code " + std::to_string((int)r));
-    t2_kernel<<<dim3((unsigned)((n + 31) / 32), (unsigned)((n + 31) / 32), (unsigned)nk), blk, 0,
-                st>>>(A, B, n, (int)nk);
+    const int zc = zhi - zlo;
+    t2_kernel<<<dim3((unsigned)((zc + 31) / 32), (unsigned)((n + 31) / 32), (unsigned)nk), blk, 0,
+                st>>>(A, B, n, (int)nk, zlo, zhi);
     HT_CUDA_TRY(cudaGetLastError(), "t2_kernel launch");
-    r = cufftExecC2C(ctx->tp_plan_n, (cufftComplex*)B, (cufftComplex*)B, CUFFT_INVERSE);
+    float2* Bz = B + (size_t)zlo * nk * n;
+    r = cufftExecC2C(ctx->tp_plan_y, (cufftComplex*)Bz, (cufftComplex*)Bz, CUFFT_INVERSE);
     if (r != CUFFT_SUCCESS) return ht_fail(HT_ERR_CUDA, "cufftExecC2C (y) failed with code " + std::to_string((int)r));
     const int m = n / 2;
     t3_pack_kernel<<<dim3((unsigned)((m / 2 + 1 + 31) / 32), (unsigned)((n + 31) / 32),
-                          (unsigned)n), blk, 0, st>>>(B, A, n, (int)nk, (const float2*)ctx->d_tw);
+                          (unsigned)zc), blk, 0, st>>>(B, A, n, (int)nk, (const float2*)ctx->d_tw,
+                                                       zlo);
     HT_CUDA_TRY(cudaGetLastError(), "t3_pack_kernel launch");
-    r = cufftExecC2C(ctx->tp_plan_m, (cufftComplex*)A, (cufftComplex*)d_out, CUFFT_INVERSE);
+    const size_t off = (size_t)zlo * n * m;   // complex elements of C and of the output
+    r = cufftExecC2C(ctx->tp_plan_x, (cufftComplex*)A + off, (cufftComplex*)d_out + off,
+                     CUFFT_INVERSE);
     if (r != CUFFT_SUCCESS) return ht_fail(HT_ERR_CUDA, "cufftExecC2C (x) failed with code " + std::to_string((int)r));
     ctx->last_kernels = 4;
     return HT_OK;
@@ -491,10 +517,13 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
 
 // ------------------------------------------------------ window + inverse FFT (tile) ----
 
-extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
-                                     double boxsize, double Rf, int wsmooth, void* stream) {
+static int smooth_tile_impl(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                            double boxsize, double Rf, int wsmooth, int zlo, int zhi,
+                            void* stream) {
     if (!ctx || !d_delta_k || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_tile: NULL argument");
     if (n < 2 || n > 4096) return ht_fail(HT_ERR_INVALID, "ht_smooth_tile: need 2 <= n <= 4096");
+    if (zlo < 0 || zhi > n || zlo >= zhi)
+        return ht_fail(HT_ERR_INVALID, "ht_smooth_tile: need 0 <= z_lo < z_hi <= n");
     int rc = check_window_args("ht_smooth_tile", boxsize, Rf);
     if (rc != HT_OK) return rc;
     if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_smooth_tile");
@@ -512,7 +541,7 @@ extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* 
         return smooth_tile_fused(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth,
                                  (cudaStream_t)stream);
     if (path == 2 && (n & 1) == 0 && (long long)n * (n / 2 + 1) < 0x7fffffffLL)
-        return smooth_tile_transposed(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth,
+        return smooth_tile_transposed(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, zlo, zhi,
                                       (cudaStream_t)stream);
     const long long nk = n / 2 + 1;
     const size_t cbytes = (size_t)nk * n * n * 2 * sizeof(float);
@@ -542,6 +571,17 @@ extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* 
         return ht_fail(HT_ERR_CUDA, "cufftExecC2R failed with code " + std::to_string((int)r));
     ctx->last_kernels = 2;
     return HT_OK;
+}
+
+extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                                     double boxsize, double Rf, int wsmooth, void* stream) {
+    return smooth_tile_impl(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, 0, n, stream);
+}
+
+extern "C" HT_API int ht_smooth_tile_planes(ht_ctx* ctx, const void* d_delta_k, float* d_out,
+                                            int n, double boxsize, double Rf, int wsmooth,
+                                            int z_lo, int z_hi, void* stream) {
+    return smooth_tile_impl(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, z_lo, z_hi, stream);
 }
 
 // ------------------------------------------------- window + inverse FFT + wrap ----

@@ -127,7 +127,7 @@ class HaloFinder:
 
     def smooth_tile(self, delta_k: torch.Tensor, n: int, boxsize: float, Rf: float,
                     wsmooth: int, out: Optional[torch.Tensor] = None,
-                    stream=None) -> torch.Tensor:
+                    stream=None, planes: Optional[tuple] = None) -> torch.Tensor:
         """ht_smooth_tile: one filter of peak_find_tile_gpu (ext/CUDAExt.jl:2984-2989) --
         window (with the 1/n^3 folded in) + out-of-place cuFFT C2R of the tile's own rfft
         straight into an n^3 float32 tile."""
@@ -138,9 +138,15 @@ class HaloFinder:
                              "view on CUDA: call .contiguous() once per tile)")
         out = torch.empty((n, n, n), dtype=torch.float32, device=delta_k.device) \
             if out is None else out
-        check(_lib.load().ht_smooth_tile(self._h, delta_k.data_ptr(),
-                                         out.data_ptr(), int(n), float(boxsize), float(Rf),
-                                         int(wsmooth), _stream_handle(stream)))
+        if planes is None:
+            check(_lib.load().ht_smooth_tile(self._h, delta_k.data_ptr(), out.data_ptr(),
+                                             int(n), float(boxsize), float(Rf), int(wsmooth),
+                                             _stream_handle(stream)))
+        else:   # only planes [lo, hi) are needed (the peak scan reads nbuff-1 .. n-nbuff)
+            check(_lib.load().ht_smooth_tile_planes(self._h, delta_k.data_ptr(),
+                                                    out.data_ptr(), int(n), float(boxsize),
+                                                    float(Rf), int(wsmooth), int(planes[0]),
+                                                    int(planes[1]), _stream_handle(stream)))
         return out
 
     def smooth_box_wrapped(self, delta_k: torch.Tensor, n: int, nbuff: int, boxsize: float,
@@ -325,9 +331,10 @@ def peak_find_tile_gpu(delta_tile, filters: Sequence, fcrits: Sequence[float], t
     ls = torch.empty_like(ds) if has_lapd else None
     for fi, (flt, fc) in enumerate(zip(filters, fcrits), start=1):
         Rf = float(flt[2])
-        finder.smooth_tile(delta_k, n, boxsize, Rf, wsmooth, out=ds)
+        planes = (int(nbuff) - 1, n - int(nbuff) + 1)   # the planes the scan reads
+        finder.smooth_tile(delta_k, n, boxsize, Rf, wsmooth, out=ds, planes=planes)
         if has_lapd:
-            finder.smooth_tile(delta_k, n, boxsize, Rf, 3, out=ls)
+            finder.smooth_tile(delta_k, n, boxsize, Rf, 3, out=ls, planes=planes)
         finder.peakfind_filter(ds, mask, nbuff, float(np.float32(fc)), fi, max_peaks, out,
                                lapd_s=ls)
     del ds, ls

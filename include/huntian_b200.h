@@ -147,6 +147,14 @@ HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, i
 HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
                           double boxsize, double Rf, int wsmooth, void* stream);
 
+/* ht_smooth_tile that needs to deliver only the planes z_lo <= k < z_hi (0-based) of the
+ * tile: the peak scan of one filter reads planes nbuff - 1 .. n - nbuff only.  The
+ * transposed path skips the other planes in its y and x passes; other planes of d_out
+ * may be left unwritten. */
+HT_API int ht_smooth_tile_planes(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                                 double boxsize, double Rf, int wsmooth, int z_lo, int z_hi,
+                                 void* stream);
+
 /* ------------------------------------------------------------ shell collapse ---- */
 
 /* Tile fields (device, Float32 column-major n1*n2*n3).  eta2* may all be NULL (1LPT:

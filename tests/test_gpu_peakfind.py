@@ -232,3 +232,19 @@ def test_fused_fft_matches_transposed_path(ht, finder, n):
     scale = np.abs(ref).max()
     assert np.abs(got - ref).max() <= 2e-6 * scale * np.log2(n ** 3)
     assert finder.device_status() == 0
+
+
+@pytest.mark.parametrize("n,lo,hi", [(44, 3, 41), (620, 53, 567)])
+def test_smooth_tile_planes(ht, finder, n, lo, hi):
+    """ht_smooth_tile_planes delivers planes [lo, hi) equal to the full transform's."""
+    import torch
+    rng = np.random.default_rng(lo)
+    a = torch.as_tensor(rng.standard_normal((n, n, n)).astype(np.float32), device="cuda")
+    ak = torch.fft.rfftn(a, dim=(0, 1, 2)).contiguous()
+    full = finder.smooth_tile(ak, n, n * 1.9, 4.0, 1).cpu().numpy()
+    part = torch.full((n, n, n), float("nan"), device="cuda")
+    finder.smooth_tile(ak, n, n * 1.9, 4.0, 1, out=part, planes=(lo, hi))
+    part = part.cpu().numpy()
+    scale = np.abs(full).max()
+    assert np.abs(part[lo:hi] - full[lo:hi]).max() <= 1e-6 * scale
+
