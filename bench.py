@@ -185,16 +185,28 @@ class Workload:
         self.tuned = {}
         if mode == "learned":
             self.model = ht.bracket.BracketModel.load(device=device)
+        self.pencil = ht.HaloFinder.pencil_supported(self.nt)
 
     def smooth(self, Rf):
         if getattr(self, "_ds", None) is None:
             self._ds = torch.empty((self.nt,) * 3, dtype=torch.float32, device=self.device)
-        # only the planes the peak scan reads: nbuff - 1 .. nt - nbuff
+        # only the planes (and, on the pencil path, the rows) the peak scan reads:
+        # nbuff - 1 .. nt - nbuff
+        lo, hi = self.nbuff - 1, self.nt - self.nbuff + 1
+        if self.pencil:
+            return self.finder.smooth_pencil(self.pk, self.nt, self.boxsize, Rf, 1, lo, hi,
+                                             out=self._ds)
         return self.finder.smooth_tile(self.dk, self.nt, self.boxsize, Rf, 1, out=self._ds,
-                                       planes=(self.nbuff - 1, self.nt - self.nbuff + 1))
+                                       planes=(lo, hi))
 
     def pf_loop(self, ev=None):
-        """Per filter: window + C2R of the tile (ht_smooth_tile), then the peak scan."""
+        """Per filter: window + inverse FFT of the tile (ht_smooth_pencil after one
+        ht_spectrum_pencil transpose at 576/1152, else ht_smooth_tile), then the peak scan."""
+        if self.pencil:
+            if getattr(self, "pk", None) is None:
+                self.pk = torch.empty((self.nt, self.nt // 2 + 1, self.nt),
+                                      dtype=torch.complex64, device=self.device)
+            self.finder.spectrum_pencil(self.dk, self.nt, out=self.pk)
         for fi, flt in enumerate(self.filters, start=1):
             ds = self.smooth(flt[2])
             if ev is not None:

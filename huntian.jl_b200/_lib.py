@@ -34,7 +34,8 @@ HT_TUNE_FFT_PATH = 4
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
            "ht_ctx_shell_r2", "ht_fsc_of_z", "ht_smooth_window", "ht_smooth_tile",
-           "ht_smooth_tile_planes",
+           "ht_smooth_tile_planes", "ht_smooth_pencil_supported", "ht_spectrum_pencil",
+           "ht_smooth_pencil",
            "ht_smooth_filter",
            "ht_peakfind_filter",
            "ht_fields_pack",
@@ -122,6 +123,12 @@ def load() -> C.CDLL:
     L.ht_smooth_tile_planes.restype = C.c_int
     L.ht_smooth_tile_planes.argtypes = [_P, _P, _P, C.c_int, dbl, dbl, C.c_int, C.c_int,
                                         C.c_int, _P]
+    L.ht_smooth_pencil_supported.restype = C.c_int
+    L.ht_smooth_pencil_supported.argtypes = [C.c_int]
+    L.ht_spectrum_pencil.restype = C.c_int
+    L.ht_spectrum_pencil.argtypes = [_P, _P, _P, C.c_int, _P]
+    L.ht_smooth_pencil.restype = C.c_int
+    L.ht_smooth_pencil.argtypes = [_P, _P, _P, C.c_int, dbl, dbl, C.c_int, C.c_int, C.c_int, _P]
     L.ht_smooth_filter.restype = C.c_int
     L.ht_smooth_filter.argtypes = [_P, _P, _P, C.c_int, C.c_int, dbl, dbl, C.c_int, _P]
     L.ht_peakfind_filter.restype = C.c_int

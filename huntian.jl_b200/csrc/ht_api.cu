@@ -447,7 +447,7 @@ extern "C" int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value) {
             ctx->tune_pf_kz = (int)value;
             return HT_OK;
         case HT_TUNE_FFT_PATH:
-            if (value < 0 || value > 3) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: FFT path must be 0..3");
+            if (value < 0 || value > 4) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: FFT path must be 0..4");
             ctx->tune_fft_path = (int)value;
             return HT_OK;
         case HT_TUNE_WALK_BPSM:

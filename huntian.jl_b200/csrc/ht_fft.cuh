@@ -126,19 +126,14 @@ struct Dft<36> {
 
 __device__ __forceinline__ int bitrev5(int l) { return __brev((unsigned)l) >> 27; }
 
-// Inverse FFT of the column col[0 .. 32 T) (shared memory, float2), in place.
+// Steps 1-3 on registers: on entry lane holds v[t] = x[lane + 32 t]; on exit v[k2] =
+// y[k2 + T k1] with k1 = bitrev5(lane).
 // twL[j] = e^{2 pi i j / (32 T)}, j < 32 T (global, cached).  w32[s] for the cross-lane
 // stages (precomputed by the caller per lane): w32[s] = e^{2 pi i (lane mod 2^s) / 2^{s+1}}.
 template <int T>
-__device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict__ twL, int lane,
-                                          const C2 (&w32)[5]) {
+__device__ __forceinline__ void warp_ifft_regs(C2 (&v)[T], const float2* __restrict__ twL,
+                                               int lane, const C2 (&w32)[5]) {
     constexpr int L = 32 * T;
-    C2 v[T];
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
-        const float2 e = col[lane + 32 * t];
-        v[t] = {e.x, e.y};
-    }
     Dft<T>::run(v);
 #pragma unroll
     for (int k2 = 1; k2 < T; ++k2) {
@@ -160,11 +155,44 @@ __device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict_
             v[k2] = upper ? hi : lo;
         }
     }
+}
+
+// Inverse FFT of the column col[0 .. 32 T) (shared memory, float2), in place, natural
+// order on input and output.
+template <int T>
+__device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict__ twL, int lane,
+                                          const C2 (&w32)[5]) {
+    C2 v[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const float2 e = col[lane + 32 * t];
+        v[t] = {e.x, e.y};
+    }
+    warp_ifft_regs<T>(v, twL, lane, w32);
     __syncwarp();
     const int k1 = bitrev5(lane);
 #pragma unroll
     for (int k2 = 0; k2 < T; ++k2) col[k2 + T * k1] = make_float2(v[k2].x, v[k2].y);
     __syncwarp();
+}
+
+// Shared-memory slot of output y[i] (i = k2 + T k1) in the "lane-major" column layout that
+// warp_ifft_store writes: slot k1 + 33 k2.  A warp's store of one k2 then covers 32
+// consecutive slots (k1 = bitrev5(lane) is a permutation), and readers walking i in order
+// step 33 slots (one bank pair) apart: both sides are free of bank conflicts.  A column
+// needs 33 T slots.
+template <int T>
+__device__ __forceinline__ int lm_slot(int i) {
+    const int k1 = i / T;
+    return k1 + 33 * (i - T * k1);
+}
+
+// Store the result of warp_ifft_regs into a lane-major column (33 T slots).
+template <int T>
+__device__ __forceinline__ void warp_ifft_store(float2* col, const C2 (&v)[T], int lane) {
+    const int k1 = bitrev5(lane);
+#pragma unroll
+    for (int k2 = 0; k2 < T; ++k2) col[k1 + 33 * k2] = make_float2(v[k2].x, v[k2].y);
 }
 
 // Per-lane cross-lane twiddles for warp_ifft: w32[st] = e^{2 pi i (lane mod 2^st) / 2^(st+1)}

@@ -137,11 +137,13 @@ __global__ void __launch_bounds__(256) t1_window_kernel(const float2* __restrict
     for (int r = ty; r < 32; r += 8) {
         const int kx = a0 + tx, kz = c0 + r;
         if (kx < NK && kz < N) {
-            const int sz = kz <= N / 2 ? kz : kz - N;
-            const float w = __ldg(tab + (kx * kx + sy * sy + sz * sz));
             float2 v = __ldg(in + ((long long)kz * N + ky) * NK + kx);
-            v.x *= w;
-            v.y *= w;
+            if (tab) {   // no table: a plain transpose (the pencil layout of the spectrum)
+                const int sz = kz <= N / 2 ? kz : kz - N;
+                const float w = __ldg(tab + (kx * kx + sy * sy + sz * sz));
+                v.x *= w;
+                v.y *= w;
+            }
             t[r][tx] = v;
         }
     }
@@ -515,6 +517,285 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
     return HT_OK;
 }
 
+// ------------------------------------------- pencil three-pass inverse FFT (n = 32 T) ----
+//
+// The spectrum of a tile is the same for every filter, so it is transposed once into
+// pencils P (ky, kx, kz), kz contiguous (ht_spectrum_pencil).  Each filter then runs three
+// passes whose loads are whole contiguous columns, one warp per column read straight into
+// registers, and whose stores leave through shared memory in pieces of 8 neighbouring
+// columns (64 bytes) in the next pass's layout:
+//   Z  window (with 1/n^3) on load, FFT along kz:  P (ky, kx, kz) -> B (kx, z, ky)
+//   Y  FFT along ky:                               B (kx, z, ky)  -> C (z, y, kx)
+//   X  half-length real packing, FFT of n/2:       C (z, y, kx)   -> out (z, y, x)
+// B holds only z in [zlo, zlo + Rz) and C only those z with y in [ylo, ylo + Ry): just the
+// output rows (z, y) in that range are written.  A peak scan of the region
+// [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.
+
+namespace {
+
+constexpr int kPencilCols = 8;   // columns (warps) per CTA in the Z and Y passes
+
+// lane-major column of 33 T slots, padded so that 8 columns start 2 banks apart
+template <int T>
+__host__ __device__ constexpr int pencil_stride() {
+    return 33 * T + (((2 - 33 * T) % 16) + 16) % 16;
+}
+
+template <int T>
+__global__ void __launch_bounds__(256) pz_kernel(const float2* __restrict__ P,
+                                                 float2* __restrict__ B, int NK, int zlo, int Rz,
+                                                 const float* __restrict__ tab,
+                                                 const float2* __restrict__ twL,
+                                                 const float2* __restrict__ tw32) {
+    constexpr int N = 32 * T, S = pencil_stride<T>();
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int ky0 = blockIdx.x * kPencilCols, kx = blockIdx.y;
+    const int ky = ky0 + w;                               // N is a multiple of 8
+    const int sy = ky <= N / 2 ? ky : ky - N;
+    const int base = kx * kx + sy * sy;
+    const float2* src = P + ((long long)ky * NK + kx) * N;
+    htfft::C2 v[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+        const int kz = lane + 32 * t;
+        const int sz = kz <= N / 2 ? kz : kz - N;
+        const float wv = __ldg(tab + (base + sz * sz));
+        const float2 e = __ldg(src + kz);
+        v[t] = {e.x * wv, e.y * wv};
+    }
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    htfft::warp_ifft_regs<T>(v, twL, lane, w32);
+    htfft::warp_ifft_store<T>(sm + w * S, v, lane);
+    __syncthreads();
+    float2* dst = B + (long long)kx * Rz * N + ky0;
+    for (int e = tid; e < kPencilCols * Rz; e += blockDim.x) {
+        const int zr = e >> 3, c = e & 7;
+        dst[(long long)zr * N + c] = sm[c * S + htfft::lm_slot<T>(zlo + zr)];
+    }
+}
+
+template <int T>
+__global__ void __launch_bounds__(256) py_kernel(const float2* __restrict__ B,
+                                                 float2* __restrict__ C, int NK, int Rz,
+                                                 int ylo, int Ry, const float2* __restrict__ twL,
+                                                 const float2* __restrict__ tw32) {
+    constexpr int N = 32 * T, S = pencil_stride<T>();
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int kx0 = blockIdx.x * kPencilCols, zr = blockIdx.y;
+    const int kx = kx0 + w;
+    if (kx < NK) {   // no barrier inside: the CTA meets at the __syncthreads below
+        const float2* src = B + ((long long)kx * Rz + zr) * N;
+        htfft::C2 v[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            const float2 e = __ldg(src + lane + 32 * t);
+            v[t] = {e.x, e.y};
+        }
+        htfft::C2 w32[5];
+        htfft::lane_twiddles(lane, tw32, w32);
+        htfft::warp_ifft_regs<T>(v, twL, lane, w32);
+        htfft::warp_ifft_store<T>(sm + w * S, v, lane);
+    }
+    __syncthreads();
+    const int ncol = min(kPencilCols, NK - kx0);
+    float2* dst = C + (long long)zr * Ry * NK + kx0;
+    for (int e = tid; e < kPencilCols * Ry; e += blockDim.x) {
+        const int yr = e >> 3, c = e & 7;
+        if (c < ncol) dst[(long long)yr * NK + c] = sm[c * S + htfft::lm_slot<T>(ylo + yr)];
+    }
+}
+
+// TH = n / 64: the packed rows have m = n / 2 = 32 TH points.  One warp per output row.
+template <int TH>
+__global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
+                                                 float2* __restrict__ out, int zlo, int ylo,
+                                                 int Ry, long long rows,
+                                                 const float2* __restrict__ twp,
+                                                 const float2* __restrict__ twM,
+                                                 const float2* __restrict__ tw32) {
+    constexpr int M = 32 * TH, N = 2 * M, NK = M + 1, S = 33 * TH;   // 33 TH >= M + 1
+    extern __shared__ float2 sm[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const long long r = (long long)blockIdx.x * (blockDim.x >> 5) + w;
+    if (r >= rows) return;   // warps are independent: no CTA barrier in this kernel
+    const int zr = (int)(r / Ry), yr = (int)(r - (long long)zr * Ry);
+    float2* col = sm + w * S;
+    const float2* src = C + r * NK;
+    for (int k = lane; k < NK; k += 32) col[k] = __ldg(src + k);
+    __syncwarp();
+    // half-length packing in place: lane handles the pair (k, M - k), k <= M / 2
+    for (int k = lane; k <= M / 2; k += 32) {
+        const float2 xa = col[k], xb = col[M - k];
+        auto pack = [&](float2 a, float2 bb, int kk) {
+            const float2 b = make_float2(bb.x, -bb.y);          // conj X[M - kk]
+            const float2 e = make_float2(a.x + b.x, a.y + b.y);
+            const float2 d = make_float2(a.x - b.x, a.y - b.y);
+            const float2 wv = __ldg(twp + kk);                  // e^{2 pi i kk / N}
+            const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
+            return make_float2(e.x - o.y, e.y + o.x);
+        };
+        const float2 zk = pack(xa, xb, k);
+        const int kh = M - k;
+        if (kh != k && kh < M) col[kh] = pack(xb, xa, kh);
+        col[k] = zk;
+    }
+    __syncwarp();
+    htfft::C2 v[TH];
+#pragma unroll
+    for (int t = 0; t < TH; ++t) {
+        const float2 e = col[lane + 32 * t];
+        v[t] = {e.x, e.y};
+    }
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
+    __syncwarp();
+    htfft::warp_ifft_store<TH>(col, v, lane);
+    __syncwarp();
+    float2* dst = out + ((long long)(zlo + zr) * N + (ylo + yr)) * M;
+#pragma unroll
+    for (int t = 0; t < TH; ++t) dst[lane + 32 * t] = col[htfft::lm_slot<TH>(lane + 32 * t)];
+}
+
+}  // namespace
+
+// Tile sides the pencil path handles: n = 32 T with T in {18, 36}.
+static bool pencil_side(int n) { return n == 576 || n == 1152; }
+
+// Z, Y and X passes from pencils P, through B and C (C may reuse P's buffer: P is read
+// only by the first pass).
+template <int T>
+static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, float2* d_out,
+                         int zlo, int zhi, int ylo, int yhi, cudaStream_t st) {
+    constexpr int n = 32 * T, TH = T / 2;
+    const int nk = n / 2 + 1, Rz = zhi - zlo, Ry = yhi - ylo;
+    const size_t smyz = (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
+    const size_t smx = (size_t)8 * 33 * TH * sizeof(float2);
+    const float2* tw = (const float2*)ctx->d_ftw;
+    const float2* twL = tw;              // e^{2 pi i j / n}, j < n (also the packing twiddles)
+    const float2* twM = tw + n;          // e^{2 pi i j / (n/2)}
+    const float2* tw32 = tw + n + n / 2;
+    HT_CUDA_TRY(cudaFuncSetAttribute(pz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "pz smem");
+    HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "py smem");
+    HT_CUDA_TRY(cudaFuncSetAttribute(px_kernel<TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "px smem");
+    pz_kernel<T><<<dim3((unsigned)(n / kPencilCols), (unsigned)nk), 256, smyz, st>>>(
+        P, B, nk, zlo, Rz, (const float*)ctx->d_win, twL, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
+    py_kernel<T><<<dim3((unsigned)((nk + kPencilCols - 1) / kPencilCols), (unsigned)Rz), 256,
+                   smyz, st>>>(B, C, nk, Rz, ylo, Ry, twL, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
+    const long long rows = (long long)Rz * Ry;
+    px_kernel<TH><<<(unsigned)((rows + 7) / 8), 256, smx, st>>>(C, d_out, zlo, ylo, Ry, rows,
+                                                                twL, twM, tw32);
+    HT_CUDA_TRY(cudaGetLastError(), "px_kernel launch");
+    return HT_OK;
+}
+
+// Window table W / n^3 per distinct integer |k|^2 (the 1/n^3 of the inverse FFT folded in).
+static int scaled_window_table(ht_ctx* ctx, int n, double boxsize, double Rf, int wsmooth,
+                               cudaStream_t st) {
+    const int h = n / 2;
+    const int nvals = 3 * h * h + 1;
+    int rc = ht_grow(&ctx->d_win, &ctx->win_bytes, (size_t)nvals * sizeof(float), "window table");
+    if (rc != HT_OK) return rc;
+    const double dk = 2.0 * 3.14159265358979323846 / boxsize;
+    window_table_kernel<<<(nvals + 255) / 256, 256, 0, st>>>((float*)ctx->d_win, nvals, dk, Rf,
+                                                             wsmooth, 1.0 / ((double)n * n * n));
+    HT_CUDA_TRY(cudaGetLastError(), "window_table_kernel launch");
+    return HT_OK;
+}
+
+// Spectrum (kz, ky, kx) -> pencils (ky, kx, kz) on stream st (the t1 transpose, no window).
+static int launch_pencil_transpose(const float2* in, float2* P, int n, cudaStream_t st) {
+    const int nk = n / 2 + 1;
+    t1_window_kernel<<<dim3((unsigned)((nk + 31) / 32), (unsigned)((n + 31) / 32), (unsigned)n),
+                       dim3(32, 8), 0, st>>>(in, P, n, nk, nullptr);
+    HT_CUDA_TRY(cudaGetLastError(), "pencil transpose launch");
+    return HT_OK;
+}
+
+// One filter from pencils P: output rows (z, y) in [zlo, zhi) x [ylo, yhi).  P may be the
+// context's first smoothing buffer (it is consumed by the first pass, which is why C can
+// take the same buffer).
+static int smooth_pencil_run(ht_ctx* ctx, const float2* P, float* d_out, int n, double boxsize,
+                             double Rf, int wsmooth, int zlo, int zhi, int ylo, int yhi,
+                             cudaStream_t st) {
+    const size_t nk = (size_t)n / 2 + 1;
+    int rc = ht_grow(&ctx->d_cwork2, &ctx->cwork2_bytes,
+                     nk * (size_t)(zhi - zlo) * n * sizeof(float2), "smoothing buffer 2");
+    if (rc == HT_OK)
+        rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes,
+                     nk * (size_t)(zhi - zlo) * (yhi - ylo) * sizeof(float2), "smoothing buffer");
+    if (rc == HT_OK) rc = fused_tables(ctx, n);
+    if (rc == HT_OK) rc = scaled_window_table(ctx, n, boxsize, Rf, wsmooth, st);
+    if (rc != HT_OK) return rc;
+    float2* B = (float2*)ctx->d_cwork2;
+    float2* C = (float2*)ctx->d_cwork;
+    float2* out = (float2*)d_out;
+    rc = n == 1152 ? launch_pencil<36>(ctx, P, B, C, out, zlo, zhi, ylo, yhi, st)
+                   : launch_pencil<18>(ctx, P, B, C, out, zlo, zhi, ylo, yhi, st);
+    if (rc != HT_OK) return rc;
+    ctx->last_kernels = 4;
+    return HT_OK;
+}
+
+// ht_smooth_tile path 4: the pencil passes behind a per-call transpose of the spectrum into
+// the context's first buffer (four HBM passes per filter instead of the transposed path's
+// six).
+static int smooth_tile_pencil(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
+                              double boxsize, double Rf, int wsmooth, int zlo, int zhi,
+                              cudaStream_t st) {
+    const size_t nk = (size_t)n / 2 + 1;
+    int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, nk * n * n * sizeof(float2),
+                     "smoothing buffer");
+    if (rc != HT_OK) return rc;
+    float2* P = (float2*)ctx->d_cwork;
+    rc = launch_pencil_transpose((const float2*)d_delta_k, P, n, st);
+    if (rc != HT_OK) return rc;
+    rc = smooth_pencil_run(ctx, P, d_out, n, boxsize, Rf, wsmooth, zlo, zhi, 0, n, st);
+    if (rc == HT_OK) ctx->last_kernels = 5;
+    return rc;
+}
+
+extern "C" HT_API int ht_smooth_pencil_supported(int n) { return pencil_side(n) ? 1 : 0; }
+
+extern "C" HT_API int ht_spectrum_pencil(ht_ctx* ctx, const void* d_delta_k, void* d_pencil,
+                                         int n, void* stream) {
+    if (!ctx || !d_delta_k || !d_pencil) return ht_fail(HT_ERR_INVALID, "ht_spectrum_pencil: NULL argument");
+    if (n < 2 || n > 4096 || (n & 1))
+        return ht_fail(HT_ERR_INVALID, "ht_spectrum_pencil: need an even n, 2 <= n <= 4096");
+    if (d_pencil == d_delta_k)
+        return ht_fail(HT_ERR_INVALID, "ht_spectrum_pencil: the transpose is out of place");
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_spectrum_pencil");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    int rc = launch_pencil_transpose((const float2*)d_delta_k, (float2*)d_pencil, n,
+                                     (cudaStream_t)stream);
+    if (rc != HT_OK) return rc;
+    ctx->last_kernels = 1;
+    return HT_OK;
+}
+
+extern "C" HT_API int ht_smooth_pencil(ht_ctx* ctx, const void* d_pencil, float* d_out, int n,
+                                       double boxsize, double Rf, int wsmooth, int lo, int hi,
+                                       void* stream) {
+    if (!ctx || !d_pencil || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_pencil: NULL argument");
+    if (!pencil_side(n))
+        return ht_fail(HT_ERR_INVALID, "ht_smooth_pencil: tile side " + std::to_string(n) +
+                                           " not supported (576 or 1152)");
+    if (lo < 0 || hi > n || lo >= hi)
+        return ht_fail(HT_ERR_INVALID, "ht_smooth_pencil: need 0 <= lo < hi <= n");
+    int rc = check_window_args("ht_smooth_pencil", boxsize, Rf);
+    if (rc != HT_OK) return rc;
+    if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_smooth_pencil");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    return smooth_pencil_run(ctx, (const float2*)d_pencil, d_out, n, boxsize, Rf, wsmooth, lo, hi,
+                             lo, hi, (cudaStream_t)stream);
+}
+
+
 // ------------------------------------------------------ window + inverse FFT (tile) ----
 
 static int smooth_tile_impl(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
@@ -528,15 +809,18 @@ static int smooth_tile_impl(ht_ctx* ctx, const void* d_delta_k, float* d_out, in
     if (rc != HT_OK) return rc;
     if (ht_fault_injected("launch")) return ht_fail(HT_ERR_FAULT, "injected launch fault: ht_smooth_tile");
     HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
-    // path: the single 3-D plan for power-of-two sides (and odd ones), the transposed
-    // 1-D pipeline otherwise; HT_TUNE_FFT_PATH overrides (1 = 3-D plan, 2 = transposed)
+    // path: the pencil passes for n = 576 and 1152, the single 3-D plan for power-of-two
+    // sides (and odd ones), the transposed 1-D pipeline otherwise; HT_TUNE_FFT_PATH
+    // overrides (1 = 3-D plan, 2 = transposed, 3 = fused, 4 = pencil).  The fused kernels
+    // read 64-byte pieces of HBM rows (20.1 ms at 1152 against 16.3 ms transposed); the
+    // pencil passes read whole columns.
     const bool pow2 = (n & (n - 1)) == 0;
-    // fused three-pass kernels: measured faster at 576 (1.84 vs 2.39 ms) but not at 1152
-    // (20.1 vs 16.3 ms: 8-column tiles read 64-byte pieces of HBM rows), so by default only
-    // there
     const bool fused_ok = n == 576 || n == 1152;
     const int path = ctx->tune_fft_path ? ctx->tune_fft_path
-                                        : (n == 576 ? 3 : (pow2 || (n & 1) ? 1 : 2));
+                                        : (pencil_side(n) ? 4 : (pow2 || (n & 1) ? 1 : 2));
+    if (path == 4 && pencil_side(n))
+        return smooth_tile_pencil(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, zlo, zhi,
+                                  (cudaStream_t)stream);
     if (path == 3 && fused_ok)
         return smooth_tile_fused(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth,
                                  (cudaStream_t)stream);

@@ -149,6 +149,43 @@ class HaloFinder:
                                                     int(planes[1]), _stream_handle(stream)))
         return out
 
+    @staticmethod
+    def pencil_supported(n: int) -> bool:
+        """Tile sides the pencil smoothing handles (576 and 1152)."""
+        return bool(_lib.load().ht_smooth_pencil_supported(int(n)))
+
+    def spectrum_pencil(self, delta_k: torch.Tensor, n: int, out: Optional[torch.Tensor] = None,
+                        stream=None) -> torch.Tensor:
+        """ht_spectrum_pencil: the tile's rfft (n, n, n//2+1) transposed once into pencils
+        (n, n//2+1, n), kz contiguous, for ht_smooth_pencil."""
+        if delta_k.dtype != torch.complex64 or tuple(delta_k.shape) != (n, n, n // 2 + 1):
+            raise ValueError("delta_k must be the complex64 rfft of an n^3 tile")
+        if not delta_k.is_contiguous():
+            raise ValueError("delta_k must be contiguous")
+        out = torch.empty((n, n // 2 + 1, n), dtype=torch.complex64, device=delta_k.device) \
+            if out is None else out
+        if out.data_ptr() == delta_k.data_ptr():
+            raise ValueError("the pencil transpose is out of place")
+        check(_lib.load().ht_spectrum_pencil(self._h, delta_k.data_ptr(), out.data_ptr(), int(n),
+                                             _stream_handle(stream)))
+        return out
+
+    def smooth_pencil(self, pencil: torch.Tensor, n: int, boxsize: float, Rf: float,
+                      wsmooth: int, lo: int, hi: int, out: Optional[torch.Tensor] = None,
+                      stream=None) -> torch.Tensor:
+        """ht_smooth_pencil: one filter of peak_find_tile_gpu from the pencil spectrum; only
+        the rows out[z, y, :] with lo <= z, y < hi are written (the rows the peak scan of
+        the inner region reads when lo = nbuff - 1, hi = n - nbuff + 1)."""
+        if pencil.dtype != torch.complex64 or tuple(pencil.shape) != (n, n // 2 + 1, n) \
+                or not pencil.is_contiguous():
+            raise ValueError("pencil must be the contiguous output of spectrum_pencil")
+        out = torch.empty((n, n, n), dtype=torch.float32, device=pencil.device) \
+            if out is None else out
+        check(_lib.load().ht_smooth_pencil(self._h, pencil.data_ptr(), out.data_ptr(), int(n),
+                                           float(boxsize), float(Rf), int(wsmooth), int(lo),
+                                           int(hi), _stream_handle(stream)))
+        return out
+
     def smooth_box_wrapped(self, delta_k: torch.Tensor, n: int, nbuff: int, boxsize: float,
                            Rf: float, wsmooth: int, out: Optional[torch.Tensor] = None,
                            stream=None) -> torch.Tensor:
@@ -326,15 +363,25 @@ def peak_find_tile_gpu(delta_tile, filters: Sequence, fcrits: Sequence[float], t
     boxsize = n * float(alatt)   # periodic tile: boxsize_local = n * alatt
     has_lapd = ioutshear >= 1
     delta_k = torch.fft.rfftn(delta, dim=(0, 1, 2)).contiguous()
+    pencil = None
+    if HaloFinder.pencil_supported(n):   # transpose the spectrum once for every filter
+        pencil = finder.spectrum_pencil(delta_k, n)
+        del delta_k
     out = HaloFinder.alloc_peaks(max_peaks, device, has_lapd)
     ds = torch.empty((n, n, n), dtype=torch.float32, device=device)
     ls = torch.empty_like(ds) if has_lapd else None
+    # the planes (and rows) the scan reads: nbuff - 1 .. n - nbuff
+    lo, hi = max(0, int(nbuff) - 1), min(n, n - int(nbuff) + 1)
     for fi, (flt, fc) in enumerate(zip(filters, fcrits), start=1):
         Rf = float(flt[2])
-        planes = (int(nbuff) - 1, n - int(nbuff) + 1)   # the planes the scan reads
-        finder.smooth_tile(delta_k, n, boxsize, Rf, wsmooth, out=ds, planes=planes)
-        if has_lapd:
-            finder.smooth_tile(delta_k, n, boxsize, Rf, 3, out=ls, planes=planes)
+        if pencil is not None:
+            finder.smooth_pencil(pencil, n, boxsize, Rf, wsmooth, lo, hi, out=ds)
+            if has_lapd:
+                finder.smooth_pencil(pencil, n, boxsize, Rf, 3, lo, hi, out=ls)
+        else:
+            finder.smooth_tile(delta_k, n, boxsize, Rf, wsmooth, out=ds, planes=(lo, hi))
+            if has_lapd:
+                finder.smooth_tile(delta_k, n, boxsize, Rf, 3, out=ls, planes=(lo, hi))
         finder.peakfind_filter(ds, mask, nbuff, float(np.float32(fc)), fi, max_peaks, out,
                                lapd_s=ls)
     del ds, ls

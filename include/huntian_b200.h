@@ -143,7 +143,8 @@ HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, i
  * FP32 once) is applied on the way into a context buffer; the inverse transform is one
  * out-of-place cuFFT C2R plan for power-of-two sides, and for other even sides three
  * batched 1-D cuFFT transforms along axes made contiguous by transposes (cuFFT's 3-D plan
- * is 3x slower there).  Plans cached per n; HT_TUNE_FFT_PATH overrides the choice. */
+ * is 3x slower there); n = 576 and 1152 transpose into pencils and run the pencil passes
+ * (ht_smooth_pencil).  Plans cached per n; HT_TUNE_FFT_PATH overrides the choice. */
 HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
                           double boxsize, double Rf, int wsmooth, void* stream);
 
@@ -154,6 +155,26 @@ HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int 
 HT_API int ht_smooth_tile_planes(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
                                  double boxsize, double Rf, int wsmooth, int z_lo, int z_hi,
                                  void* stream);
+
+/* Pencil form of the per-filter tile smoothing, for tile sides n = 576 and 1152
+ * (ht_smooth_pencil_supported(n) != 0).  The rfft of the tile is the same for every
+ * filter, so it is transposed once into pencils:
+ *   ht_spectrum_pencil: d_pencil (complex64, (n, n/2+1, n) column-major) receives
+ *     P[kz, kx, ky] = d_delta_k[kx, ky, kz] (d_delta_k as for ht_smooth_tile; out of
+ *     place, any even n).
+ *   ht_smooth_pencil: for one filter, the same irfft(W . delta_k) / n^3 as ht_smooth_tile,
+ *     computed in three passes (window + FFT along kz, FFT along ky, half-length real FFT
+ *     along kx), each reading whole contiguous columns; only the rows d_out[:, j, k] with
+ *     lo <= j - 1, k - 1 < hi (1-based j, k) are written: the rows that the peak scan of the
+ *     inner region [lo + 1, hi - 1) reads (lo = nbuff - 1, hi = n - nbuff + 1).
+ * These replace the per-filter copy + window + irfft of ext/CUDAExt.jl:2951-2989 when the
+ * spectrum is kept across filters (peak_find_tile_gpu's loop over filters). */
+HT_API int ht_smooth_pencil_supported(int n);
+HT_API int ht_spectrum_pencil(ht_ctx* ctx, const void* d_delta_k, void* d_pencil, int n,
+                              void* stream);
+HT_API int ht_smooth_pencil(ht_ctx* ctx, const void* d_pencil, float* d_out, int n,
+                            double boxsize, double Rf, int wsmooth, int lo, int hi,
+                            void* stream);
 
 /* ------------------------------------------------------------ shell collapse ---- */
 
@@ -270,11 +291,12 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
  *                       cost inside a block (default 17);
  *   HT_TUNE_PF_KZ       peak scan: k-planes per CTA (0 = chosen from the grid size);
  *   HT_TUNE_WALK_BPSM   shell walk: resident blocks per SM (0 = the occupancy maximum);
- *   HT_TUNE_FFT_PATH    ht_smooth_tile's inverse FFT: 0 = by tile side (one 3-D cuFFT plan
- *                       for powers of two, the fused three-pass kernels at 576, otherwise
+ *   HT_TUNE_FFT_PATH    ht_smooth_tile's inverse FFT: 0 = by tile side (the pencil passes
+ *                       at 576 and 1152, one 3-D cuFFT plan for powers of two, otherwise
  *                       transposes + batched 1-D transforms), 1 = 3-D plan, 2 = transposed
- *                       1-D (even sides), 3 = fused (sides 576 and 1152).  They differ by FP32
- *                       round-off, so keep one choice per run for reproducible peaks. */
+ *                       1-D (even sides), 3 = fused (sides 576 and 1152), 4 = pencil (sides
+ *                       576 and 1152).  They differ by FP32 round-off, so keep one choice per
+ *                       run for reproducible peaks. */
 #define HT_TUNE_BLOCK_BITS 1
 #define HT_TUNE_PF_KZ 2
 #define HT_TUNE_WALK_BPSM 3

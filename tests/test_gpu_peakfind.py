@@ -234,6 +234,72 @@ def test_fused_fft_matches_transposed_path(ht, finder, n):
     assert finder.device_status() == 0
 
 
+@pytest.mark.parametrize("n,wsmooth", [(576, 1), (576, 0), (576, 3), (1152, 1)])
+def test_pencil_fft_matches_transposed_path(ht, finder, n, wsmooth):
+    """The pencil passes (spectrum transposed once to kz-contiguous pencils, then window +
+    FFT along kz, FFT along ky, half-length real FFT along kx, each pass reading whole
+    columns) against the transposed cuFFT path (itself checked against FP64 above), both
+    as ht_smooth_pencil on the full range and as ht_smooth_tile's path 4."""
+    import torch
+    rng = np.random.default_rng(n + wsmooth)
+    a = torch.as_tensor(rng.standard_normal((n, n, n)).astype(np.float32), device="cuda")
+    ak = torch.fft.rfftn(a, dim=(0, 1, 2)).contiguous()
+    del a
+    box, Rf = n * 1.46, 6.0
+    try:
+        finder.tune(fft_path=2)
+        ref = finder.smooth_tile(ak, n, box, Rf, wsmooth)
+        finder.tune(fft_path=4)
+        via_tile = finder.smooth_tile(ak, n, box, Rf, wsmooth)
+    finally:
+        finder.tune(fft_path=0)
+    pk = finder.spectrum_pencil(ak, n)
+    got = finder.smooth_pencil(pk, n, box, Rf, wsmooth, 0, n)
+    torch.cuda.synchronize()
+    scale = float(ref.abs().max())
+    tol = 2e-6 * scale * np.log2(n ** 3)
+    assert float((got - ref).abs().max()) <= tol
+    assert torch.equal(got, via_tile)      # same kernels, same order: bit-identical
+    assert finder.device_status() == 0
+
+
+@pytest.mark.parametrize("n,lo,hi", [(576, 63, 513), (1152, 63, 1089)])
+def test_pencil_region_rows(ht, finder, n, lo, hi):
+    """ht_smooth_pencil(lo, hi) writes exactly the rows (z, y) in [lo, hi)^2, equal to the
+    full transform's, and leaves every other row of the output untouched."""
+    import torch
+    rng = np.random.default_rng(hi)
+    a = torch.as_tensor(rng.standard_normal((n, n, n)).astype(np.float32), device="cuda")
+    ak = torch.fft.rfftn(a, dim=(0, 1, 2)).contiguous()
+    del a
+    pk = finder.spectrum_pencil(ak, n)
+    del ak
+    full = finder.smooth_pencil(pk, n, n * 1.9, 4.0, 1, 0, n)
+    part = torch.full((n, n, n), float("nan"), device="cuda")
+    finder.smooth_pencil(pk, n, n * 1.9, 4.0, 1, lo, hi, out=part)
+    torch.cuda.synchronize()
+    assert torch.equal(part[lo:hi, lo:hi], full[lo:hi, lo:hi])
+    written = ~torch.isnan(part).all(dim=2)
+    expect = torch.zeros((n, n), dtype=torch.bool, device="cuda")
+    expect[lo:hi, lo:hi] = True
+    assert torch.equal(written, expect)
+    assert not torch.isnan(part[lo:hi, lo:hi]).any()
+
+
+def test_pencil_rejects_bad_arguments(ht, finder):
+    import torch
+    assert ht.HaloFinder.pencil_supported(576) and ht.HaloFinder.pencil_supported(1152)
+    assert not ht.HaloFinder.pencil_supported(620)
+    pk = torch.zeros((4, 3, 4), dtype=torch.complex64, device="cuda")
+    with pytest.raises(ValueError):
+        finder.smooth_pencil(pk, 576, 100.0, 4.0, 1, 0, 576)
+    big = torch.zeros((2, 2, 2), dtype=torch.complex64, device="cuda")
+    with pytest.raises(ht.HTError):   # side 620 has no pencil passes: reported, not run
+        ht._lib.check(ht._lib.load().ht_smooth_pencil(finder.handle, big.data_ptr(),
+                                                      big.data_ptr(), 620, 100.0, 4.0, 1, 0,
+                                                      620, None))
+
+
 @pytest.mark.parametrize("n,lo,hi", [(44, 3, 41), (620, 53, 567)])
 def test_smooth_tile_planes(ht, finder, n, lo, hi):
     """ht_smooth_tile_planes delivers planes [lo, hi) equal to the full transform's."""
