@@ -4,13 +4,13 @@
 //
 // Four-step with L = 32 x T (Bailey 1990): lane l (0..31) owns x[l + 32 t], t = 0..T-1.
 //   1. each lane: T-point DFT over t in registers (mixed radix 2/3/4, composed),
-//   2. twiddle by e^{2 pi i l k2 / L},
+//   2. twiddle by e^{2 pi i l k2 / L} (read from a lane-major table: coalesced),
 //   3. for every k2: 32-point DFT across the lanes with xor shuffles (radix-2,
 //      decimation in frequency: lane l ends with index k1 = bitrev5(l)),
 //   4. y[k2 + T k1] goes back to the column.
 // Small-DFT twiddles come from __constant__ tables of e^{2 pi i j / N} computed on the host
 // in FP64 (fused_tables in ht_smooth.cu); the lane-dependent step-2 twiddles from a per-L
-// global table.
+// global table laid out [k2][lane], so that a warp reads 256 contiguous bytes per k2.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -128,31 +128,35 @@ __device__ __forceinline__ int bitrev5(int l) { return __brev((unsigned)l) >> 27
 
 // Steps 1-3 on registers: on entry lane holds v[t] = x[lane + 32 t]; on exit v[k2] =
 // y[k2 + T k1] with k1 = bitrev5(lane).
-// twL[j] = e^{2 pi i j / (32 T)}, j < 32 T (global, cached).  w32[s] for the cross-lane
-// stages (precomputed by the caller per lane): w32[s] = e^{2 pi i (lane mod 2^s) / 2^{s+1}}.
+// twLM[32 k2 + l] = e^{2 pi i l k2 / (32 T)}, k2 < T, l < 32 (global, cached).  w32[s] for
+// the cross-lane stages (precomputed by the caller per lane):
+// w32[s] = e^{2 pi i (lane mod 2^s) / 2^{s+1}}.
 template <int T>
-__device__ __forceinline__ void warp_ifft_regs(C2 (&v)[T], const float2* __restrict__ twL,
+__device__ __forceinline__ void warp_ifft_regs(C2 (&v)[T], const float2* __restrict__ twLM,
                                                int lane, const C2 (&w32)[5]) {
-    constexpr int L = 32 * T;
     Dft<T>::run(v);
 #pragma unroll
     for (int k2 = 1; k2 < T; ++k2) {
-        const float2 w = __ldg(twL + (lane * k2) % L);
+        const float2 w = __ldg(twLM + 32 * k2 + lane);
         v[k2] = mul(v[k2], {w.x, w.y});
     }
     // 32-point DFT across lanes, decimation in frequency: spans 16, 8, 4, 2, 1
 #pragma unroll
+    // Lower lane: a + b; upper lane: (b - a) w_{2s}^{lane mod s}, written as one signed sum
+    // b + sg a and a product by we (1 on lower lanes, and on every lane of the last stage,
+    // where w_2^0 = 1): the same roundings as the two-branch form, a third of the work.
     for (int st = 4; st >= 0; --st) {
         const int s = 1 << st;
         const bool upper = (lane & s) != 0;
+        const float sg = upper ? -1.f : 1.f;
+        const C2 we = upper ? w32[st] : C2{1.f, 0.f};
 #pragma unroll
         for (int k2 = 0; k2 < T; ++k2) {
-            C2 a = v[k2];
-            C2 b = {__shfl_xor_sync(0xffffffffu, a.x, s), __shfl_xor_sync(0xffffffffu, a.y, s)};
-            // lower lane: a + b; upper lane: (b - a) * w_{2s}^{lane mod s}
-            const C2 lo = add(a, b);
-            const C2 hi = mul(sub(b, a), w32[st]);
-            v[k2] = upper ? hi : lo;
+            const C2 a = v[k2];
+            const C2 b = {__shfl_xor_sync(0xffffffffu, a.x, s),
+                          __shfl_xor_sync(0xffffffffu, a.y, s)};
+            const C2 r = {fmaf(sg, a.x, b.x), fmaf(sg, a.y, b.y)};
+            v[k2] = st == 0 ? r : mul(r, we);
         }
     }
 }
@@ -160,7 +164,7 @@ __device__ __forceinline__ void warp_ifft_regs(C2 (&v)[T], const float2* __restr
 // Inverse FFT of the column col[0 .. 32 T) (shared memory, float2), in place, natural
 // order on input and output.
 template <int T>
-__device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict__ twL, int lane,
+__device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict__ twLM, int lane,
                                           const C2 (&w32)[5]) {
     C2 v[T];
 #pragma unroll
@@ -168,7 +172,7 @@ __device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict_
         const float2 e = col[lane + 32 * t];
         v[t] = {e.x, e.y};
     }
-    warp_ifft_regs<T>(v, twL, lane, w32);
+    warp_ifft_regs<T>(v, twLM, lane, w32);
     __syncwarp();
     const int k1 = bitrev5(lane);
 #pragma unroll
@@ -177,22 +181,25 @@ __device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict_
 }
 
 // Shared-memory slot of output y[i] (i = k2 + T k1) in the "lane-major" column layout that
-// warp_ifft_store writes: slot k1 + 33 k2.  A warp's store of one k2 then covers 32
-// consecutive slots (k1 = bitrev5(lane) is a permutation), and readers walking i in order
-// step 33 slots (one bank pair) apart: both sides are free of bank conflicts.  A column
-// needs 33 T slots.
+// warp_ifft_store writes: slot rot(k1) + 33 k2, rot(k1) = (k1 >> 1) | ((k1 & 1) << 4).  A
+// warp's store of one k2 covers 32 consecutive slots, and each half-warp (even k1 in lanes
+// 0-15, odd k1 in lanes 16-31, as k1 = bitrev5(lane)) 16 consecutive ones; readers walking i
+// in order step 33 slots (one bank pair) apart: both sides are free of bank conflicts for
+// 8-byte elements.  A column needs 33 T slots.
+__device__ __forceinline__ int lm_rot(int k1) { return (k1 >> 1) | ((k1 & 1) << 4); }
+
 template <int T>
 __device__ __forceinline__ int lm_slot(int i) {
     const int k1 = i / T;
-    return k1 + 33 * (i - T * k1);
+    return lm_rot(k1) + 33 * (i - T * k1);
 }
 
 // Store the result of warp_ifft_regs into a lane-major column (33 T slots).
 template <int T>
 __device__ __forceinline__ void warp_ifft_store(float2* col, const C2 (&v)[T], int lane) {
-    const int k1 = bitrev5(lane);
+    const int s = lm_rot(bitrev5(lane));
 #pragma unroll
-    for (int k2 = 0; k2 < T; ++k2) col[k1 + 33 * k2] = make_float2(v[k2].x, v[k2].y);
+    for (int k2 = 0; k2 < T; ++k2) col[s + 33 * k2] = make_float2(v[k2].x, v[k2].y);
 }
 
 // Per-lane cross-lane twiddles for warp_ifft: w32[st] = e^{2 pi i (lane mod 2^st) / 2^(st+1)}

@@ -30,6 +30,7 @@
 
 #include <mutex>
 
+#include "ht_async.cuh"
 #include "ht_internal.cuh"
 
 namespace {
@@ -122,18 +123,10 @@ constexpr int kStages = 4;                 // stages in flight per CTA (8 planes
 constexpr int kPlaneFloats = kBoxX * kBoxY;                // 1360
 constexpr int kPlaneBytes = kPlaneFloats * 4 * kPPS;       // bytes of one stage's copy
 constexpr int kSlotFloats = 2720;          // 10880 B per stage: 128-byte aligned slots
-constexpr long long kWaitNs = 2000000000LL;  // bounded mbarrier wait: 2 s
 static_assert(kPlaneFloats * kPPS <= kSlotFloats && (kSlotFloats * 4) % 128 == 0, "slot size");
 
-__device__ __forceinline__ unsigned smem_addr(const void* p) {
-    return (unsigned)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ long long global_ns() {
-    long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
+using htasync::bar_wait;
+using htasync::smem_addr;
 
 __device__ __forceinline__ void tma_plane(float* dst, const CUtensorMap* tm, int x, int y,
                                           int z, unsigned long long* bar) {
@@ -144,22 +137,6 @@ __device__ __forceinline__ void tma_plane(float* dst, const CUtensorMap* tm, int
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
         "[%0], [%1, {%2, %3, %4}], [%5];"
         :: "r"(smem_addr(dst)), "l"(tm), "r"(x), "r"(y), "r"(z), "r"(b) : "memory");
-}
-
-// Wait for phase `parity` of the barrier, giving up after kWaitNs.
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
-    const unsigned b = smem_addr(bar);
-    long long t0 = 0;
-    for (int it = 0;; ++it) {
-        unsigned ok;
-        asm volatile("{\n .reg .pred p;\n"
-                     " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-                     " selp.u32 %0, 1, 0, p;\n}"
-                     : "=r"(ok) : "r"(b), "r"(parity) : "memory");
-        if (ok) return true;
-        if (it == 0) t0 = global_ns();
-        else if ((it & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
-    }
 }
 
 // One CTA: 32 (i) x 32 (j) cells over kz planes; thread (tx, ty) owns column i = ib + tx

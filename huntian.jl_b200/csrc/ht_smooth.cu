@@ -6,11 +6,13 @@
 // and the modes are multiplied by Float32(W) from it (second kernel, bandwidth-bound:
 // 8 B read + 8 B written per mode).  k = 0 is left unchanged, as in the reference.
 #include <cufft.h>
+#include <algorithm>
 #include <math.h>
 
 #include <string>
 #include <vector>
 
+#include "ht_async.cuh"
 #include "ht_fft.cuh"
 #include "ht_internal.cuh"
 
@@ -439,17 +441,34 @@ __global__ void __launch_bounds__(256) fft_x_kernel(const float2* __restrict__ B
 
 }  // namespace
 
-// Twiddle tables of the fused path for side n (FP64 on the host, stored as FP32).
+// Twiddle tables of the fused and pencil paths for side n (FP64 on the host, stored as
+// FP32), at these offsets of ctx->d_ftw (fused_tw):
+//   0         e^{2 pi i j / n}, j < n (natural order: the real-packing twiddles)
+//   n         e^{2 pi i j / 32}, j < 32 (the cross-lane stages)
+//   n + 32    e^{2 pi i l k2 / n} at [32 k2 + l], k2 < n/32 (warp FFT step 2, lane-major)
+//   2 n + 32  e^{2 pi i l k2 / (n/2)} at [32 k2 + l], k2 < n/64 (the half-length FFT)
+struct FusedTw {
+    const float2 *nat, *w32, *lmL, *lmM;
+};
+static FusedTw fused_tw(const ht_ctx* ctx, int n) {
+    const float2* t = (const float2*)ctx->d_ftw;
+    return {t, t + n, t + n + 32, t + 2 * n + 32};
+}
+
 static int fused_tables(ht_ctx* ctx, int n) {
     if (ctx->fz_n == n) return HT_OK;
-    std::vector<float2> t((size_t)n + n / 2 + 32);
+    std::vector<float2> t((size_t)n + 32 + n + n / 2);
     auto w = [](double j, double N) {
         const double ph = 2.0 * 3.14159265358979323846 * j / N;
         return make_float2((float)cos(ph), (float)sin(ph));
     };
-    for (int j = 0; j < n; ++j) t[j] = w(j, n);               // e^{2 pi i j / n}
-    for (int j = 0; j < n / 2; ++j) t[n + j] = w(j, n / 2);   // e^{2 pi i j / (n/2)}
-    for (int j = 0; j < 32; ++j) t[n + n / 2 + j] = w(j, 32);
+    for (int j = 0; j < n; ++j) t[j] = w(j, n);
+    for (int j = 0; j < 32; ++j) t[n + j] = w(j, 32);
+    const size_t oL = (size_t)n + 32, oM = (size_t)2 * n + 32;
+    for (int k2 = 0; k2 < n / 32; ++k2)
+        for (int l = 0; l < 32; ++l) t[oL + 32 * k2 + l] = w((double)l * k2, n);
+    for (int k2 = 0; k2 < n / 64; ++k2)
+        for (int l = 0; l < 32; ++l) t[oM + 32 * k2 + l] = w((double)l * k2, n / 2);
     int rc = ht_grow(&ctx->d_ftw, &ctx->ftw_bytes, t.size() * sizeof(float2), "FFT twiddles");
     if (rc != HT_OK) return rc;
     HT_CUDA_TRY(cudaMemcpy(ctx->d_ftw, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice),
@@ -471,10 +490,10 @@ static int launch_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, cudaSt
     const int nk = n / 2 + 1, m = n / 2;
     const size_t smz = (size_t)kFftCols * (n + 1) * sizeof(float2);
     const size_t smx = (size_t)kFftCols * (m + 2) * sizeof(float2);
-    const float2* tw = (const float2*)ctx->d_ftw;
-    const float2* twL = tw;              // n
-    const float2* twM = tw + n;          // n / 2
-    const float2* tw32 = tw + n + n / 2;
+    const FusedTw tw = fused_tw(ctx, n);
+    const float2* twL = tw.lmL;
+    const float2* twM = tw.lmM;
+    const float2* tw32 = tw.w32;
     HT_CUDA_TRY(cudaFuncSetAttribute(fft_z_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz), "fft_z smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(fft_y_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz), "fft_y smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(fft_x_kernel<T / 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "fft_x smem");
@@ -521,15 +540,21 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
 //
 // The spectrum of a tile is the same for every filter, so it is transposed once into
 // pencils P (ky, kx, kz), kz contiguous (ht_spectrum_pencil).  Each filter then runs three
-// passes whose loads are whole contiguous columns, one warp per column read straight into
-// registers, and whose stores leave through shared memory in pieces of 8 neighbouring
-// columns (64 bytes) in the next pass's layout:
-//   Z  window (with 1/n^3) on load, FFT along kz:  P (ky, kx, kz) -> B (kx, z, ky)
-//   Y  FFT along ky:                               B (kx, z, ky)  -> C (z, y, kx)
-//   X  half-length real packing, FFT of n/2:       C (z, y, kx)   -> out (z, y, x)
+// passes:
+//   Z  window (with 1/n^3), FFT along kz:        P (ky, kx, kz) -> B (kx, z, ky)
+//   Y  FFT along ky:                             B (kx, z, ky)  -> C (z, y, kx)
+//   X  half-length real packing, FFT of n/2:     C (z, y, kx)   -> out (z, y, x)
 // B holds only z in [zlo, zlo + Rz) and C only those z with y in [ylo, ylo + Ry): just the
 // output rows (z, y) in that range are written.  A peak scan of the region
-// [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.
+// [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.  C rows carry one pad
+// element (n/2 + 2 complex values) so that every row starts on 16 bytes.
+//
+// All three kernels are persistent and software-pipelined: the next work item's columns
+// arrive by 1-D bulk copies (cp.async.bulk, completing on an mbarrier) while the current
+// one is transformed.  Z and Y: a CTA takes 8 neighbouring columns (8 warps, one column
+// each), reads them from shared memory into registers, issues the next item's copies,
+// transforms, and stores the 8 results through shared memory in 64-byte pieces of the
+// next layout.  X: every warp streams rows with a two-slot ring of its own.
 
 namespace {
 
@@ -541,123 +566,285 @@ __host__ __device__ constexpr int pencil_stride() {
     return 33 * T + (((2 - 33 * T) % 16) + 16) % 16;
 }
 
+// Z / Y shared memory: 8 input columns (bulk-copy destination) + 8 lane-major outputs
 template <int T>
-__global__ void __launch_bounds__(256) pz_kernel(const float2* __restrict__ P,
-                                                 float2* __restrict__ B, int NK, int zlo, int Rz,
-                                                 const float* __restrict__ tab,
-                                                 const float2* __restrict__ twL,
-                                                 const float2* __restrict__ tw32) {
-    constexpr int N = 32 * T, S = pencil_stride<T>();
-    extern __shared__ float2 sm[];
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int ky0 = blockIdx.x * kPencilCols, kx = blockIdx.y;
-    const int ky = ky0 + w;                               // N is a multiple of 8
-    const int sy = ky <= N / 2 ? ky : ky - N;
-    const int base = kx * kx + sy * sy;
-    const float2* src = P + ((long long)ky * NK + kx) * N;
-    htfft::C2 v[T];
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
-        const int kz = lane + 32 * t;
-        const int sz = kz <= N / 2 ? kz : kz - N;
-        const float wv = __ldg(tab + (base + sz * sz));
-        const float2 e = __ldg(src + kz);
-        v[t] = {e.x * wv, e.y * wv};
-    }
-    htfft::C2 w32[5];
-    htfft::lane_twiddles(lane, tw32, w32);
-    htfft::warp_ifft_regs<T>(v, twL, lane, w32);
-    htfft::warp_ifft_store<T>(sm + w * S, v, lane);
-    __syncthreads();
-    float2* dst = B + (long long)kx * Rz * N + ky0;
-    for (int e = tid; e < kPencilCols * Rz; e += blockDim.x) {
-        const int zr = e >> 3, c = e & 7;
-        dst[(long long)zr * N + c] = sm[c * S + htfft::lm_slot<T>(zlo + zr)];
+constexpr size_t pencil_smem_yz() {
+    return (size_t)kPencilCols * (32 * T + pencil_stride<T>()) * sizeof(float2);
+}
+
+// X: a warp's slot holds 33 TH complex values rounded up to even (16-byte slots; a padded
+// C row of M + 2 values fits), two slots per warp
+template <int TH>
+__host__ __device__ constexpr int pencil_slot_x() {
+    return (33 * TH + 1) & ~1;
+}
+template <int TH>
+constexpr size_t pencil_smem_x() {
+    return (size_t)8 * 2 * pencil_slot_x<TH>() * sizeof(float2);
+}
+
+// Transposed store of the CTA's 8 lane-major columns: dst[r * pitch + c] = column c's
+// output lo + r, for r < R and c < ncol.
+template <int T, int S>
+__device__ __forceinline__ void pencil_store(const float2* __restrict__ ob, float2* dst,
+                                             long long pitch, int lo, int R, int ncol,
+                                             int tid) {
+    for (int e = tid; e < kPencilCols * R; e += 256) {
+        const int r = e >> 3, c = e & 7;
+        if (c < ncol) dst[(long long)r * pitch + c] = ob[c * S + htfft::lm_slot<T>(lo + r)];
     }
 }
 
 template <int T>
-__global__ void __launch_bounds__(256) py_kernel(const float2* __restrict__ B,
-                                                 float2* __restrict__ C, int NK, int Rz,
-                                                 int ylo, int Ry, const float2* __restrict__ twL,
-                                                 const float2* __restrict__ tw32) {
-    constexpr int N = 32 * T, S = pencil_stride<T>();
-    extern __shared__ float2 sm[];
+__global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P,
+                                                    float2* __restrict__ B, int NK, int zlo,
+                                                    int Rz, const float* __restrict__ tab,
+                                                    const float2* __restrict__ twL,
+                                                    const float2* __restrict__ tw32,
+                                                    int32_t* __restrict__ status) {
+    constexpr int N = 32 * T, S = pencil_stride<T>(), NB = N / kPencilCols, H = T / 2;
+    extern __shared__ __align__(128) float2 sm[];
+    float2* in = sm;                          // 8 columns of N
+    float2* ob = sm + kPencilCols * N;        // 8 lane-major columns of S
+    __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int kx0 = blockIdx.x * kPencilCols, zr = blockIdx.y;
-    const int kx = kx0 + w;
-    if (kx < NK) {   // no barrier inside: the CTA meets at the __syncthreads below
-        const float2* src = B + ((long long)kx * Rz + zr) * N;
+    const int ntasks = NK * NB;               // task = kx * NB + ky block
+    if (tid == 0) {
+        htasync::bar_init(&bar, 1);
+        htasync::bar_init_fence();
+    }
+    __syncthreads();
+    auto issue = [&](int tk) {                // thread 0
+        const int kx = tk / NB, ky0 = (tk - kx * NB) * kPencilCols;
+        htasync::bar_expect(&bar, kPencilCols * N * (unsigned)sizeof(float2));
+        for (int c = 0; c < kPencilCols; ++c)
+            htasync::bulk_load(in + c * N, P + ((long long)(ky0 + c) * NK + kx) * N,
+                               N * (unsigned)sizeof(float2), &bar);
+    };
+    int task = blockIdx.x;
+    if (tid == 0 && task < ntasks) issue(task);
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    unsigned parity = 0;
+    bool ok = true;
+    for (; task < ntasks; task += gridDim.x) {
+        const int kx = task / NB, ky0 = (task - kx * NB) * kPencilCols, ky = ky0 + w;
+        // Window W(base + sz^2), gathered before the wait (scattered L2 reads that do not
+        // depend on the copy).  Each value is fetched once: kz = lane + 32 t < N/2 for
+        // t < H; the upper half kz' = N - kz (same sz^2) is lane 32 - lane's value at
+        // t' = T - 1 - t, handed over by a shuffle.  Lane 0's upper half kz = 32 t has
+        // |sz| = 32 (T - t): its own lower-half value, or N/2 (wmid) at t = H.
+        const int sy = ky <= N / 2 ? ky : ky - N;
+        const int base = kx * kx + sy * sy;
+        float wl[H];
+#pragma unroll
+        for (int t = 0; t < H; ++t) {
+            const int kz = lane + 32 * t;
+            wl[t] = __ldg(tab + (base + kz * kz));
+        }
+        const float wmid = __ldg(tab + (base + (N / 2) * (N / 2)));
+        ok = htasync::bar_wait(&bar, parity);
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+        parity ^= 1;
         htfft::C2 v[T];
+        const float2* col = in + w * N;
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-            const float2 e = __ldg(src + lane + 32 * t);
+            const float2 e = col[lane + 32 * t];
             v[t] = {e.x, e.y};
         }
-        htfft::C2 w32[5];
-        htfft::lane_twiddles(lane, tw32, w32);
+        __syncthreads();                      // every column is in registers: refill `in`
+        if (tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
+#pragma unroll
+        for (int t = 0; t < T; ++t) {
+            float wv;
+            if (t < H) {
+                wv = wl[t];
+            } else {
+                const float sh = __shfl_sync(0xffffffffu, wl[T - 1 - t], (32 - lane) & 31);
+                const float own = t == H ? wmid : wl[(T - t) % H];
+                wv = lane == 0 ? own : sh;
+            }
+            v[t].x *= wv;
+            v[t].y *= wv;
+        }
         htfft::warp_ifft_regs<T>(v, twL, lane, w32);
-        htfft::warp_ifft_store<T>(sm + w * S, v, lane);
+        htfft::warp_ifft_store<T>(ob + w * S, v, lane);
+        __syncthreads();
+        pencil_store<T, S>(ob, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, kPencilCols, tid);
     }
-    __syncthreads();
-    const int ncol = min(kPencilCols, NK - kx0);
-    float2* dst = C + (long long)zr * Ry * NK + kx0;
-    for (int e = tid; e < kPencilCols * Ry; e += blockDim.x) {
-        const int yr = e >> 3, c = e & 7;
-        if (c < ncol) dst[(long long)yr * NK + c] = sm[c * S + htfft::lm_slot<T>(ylo + yr)];
+    if (!ok && tid == 0) {
+        // record the timeout, then wait (bounded) for the copy still in flight
+        atomicExch(status, 1);
+        htasync::bar_wait(&bar, parity);
     }
 }
 
-// TH = n / 64: the packed rows have m = n / 2 = 32 TH points.  One warp per output row.
-template <int TH>
-__global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
-                                                 float2* __restrict__ out, int zlo, int ylo,
-                                                 int Ry, long long rows,
-                                                 const float2* __restrict__ twp,
-                                                 const float2* __restrict__ twM,
-                                                 const float2* __restrict__ tw32) {
-    constexpr int M = 32 * TH, N = 2 * M, NK = M + 1, S = 33 * TH;   // 33 TH >= M + 1
-    extern __shared__ float2 sm[];
+template <int T>
+__global__ void __launch_bounds__(256, 1) py_kernel(const float2* __restrict__ B,
+                                                    float2* __restrict__ C, int NK, int NKP,
+                                                    int Rz, int ylo, int Ry,
+                                                    const float2* __restrict__ twL,
+                                                    const float2* __restrict__ tw32,
+                                                    int32_t* __restrict__ status) {
+    constexpr int N = 32 * T, S = pencil_stride<T>();
+    extern __shared__ __align__(128) float2 sm[];
+    float2* in = sm;
+    float2* ob = sm + kPencilCols * N;
+    __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const long long r = (long long)blockIdx.x * (blockDim.x >> 5) + w;
-    if (r >= rows) return;   // warps are independent: no CTA barrier in this kernel
-    const int zr = (int)(r / Ry), yr = (int)(r - (long long)zr * Ry);
-    float2* col = sm + w * S;
-    const float2* src = C + r * NK;
-    for (int k = lane; k < NK; k += 32) col[k] = __ldg(src + k);
-    __syncwarp();
-    // half-length packing in place: lane handles the pair (k, M - k), k <= M / 2
-    for (int k = lane; k <= M / 2; k += 32) {
-        const float2 xa = col[k], xb = col[M - k];
-        auto pack = [&](float2 a, float2 bb, int kk) {
-            const float2 b = make_float2(bb.x, -bb.y);          // conj X[M - kk]
-            const float2 e = make_float2(a.x + b.x, a.y + b.y);
-            const float2 d = make_float2(a.x - b.x, a.y - b.y);
-            const float2 wv = __ldg(twp + kk);                  // e^{2 pi i kk / N}
-            const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
-            return make_float2(e.x - o.y, e.y + o.x);
-        };
-        const float2 zk = pack(xa, xb, k);
-        const int kh = M - k;
-        if (kh != k && kh < M) col[kh] = pack(xb, xa, kh);
-        col[k] = zk;
+    const int NKB = (NK + kPencilCols - 1) / kPencilCols;
+    const int ntasks = Rz * NKB;              // task = zr * NKB + kx block
+    if (tid == 0) {
+        htasync::bar_init(&bar, 1);
+        htasync::bar_init_fence();
     }
-    __syncwarp();
-    htfft::C2 v[TH];
-#pragma unroll
-    for (int t = 0; t < TH; ++t) {
-        const float2 e = col[lane + 32 * t];
-        v[t] = {e.x, e.y};
-    }
+    __syncthreads();
+    auto issue = [&](int tk) {                // thread 0
+        const int zr = tk / NKB, kx0 = (tk - zr * NKB) * kPencilCols;
+        const int ncol = min(kPencilCols, NK - kx0);
+        htasync::bar_expect(&bar, ncol * N * (unsigned)sizeof(float2));
+        for (int c = 0; c < ncol; ++c)
+            htasync::bulk_load(in + c * N, B + ((long long)(kx0 + c) * Rz + zr) * N,
+                               N * (unsigned)sizeof(float2), &bar);
+    };
+    int task = blockIdx.x;
+    if (tid == 0 && task < ntasks) issue(task);
     htfft::C2 w32[5];
     htfft::lane_twiddles(lane, tw32, w32);
-    htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
-    __syncwarp();
-    htfft::warp_ifft_store<TH>(col, v, lane);
-    __syncwarp();
-    float2* dst = out + ((long long)(zlo + zr) * N + (ylo + yr)) * M;
+    unsigned parity = 0;
+    bool ok = true;
+    for (; task < ntasks; task += gridDim.x) {
+        const int zr = task / NKB, kx0 = (task - zr * NKB) * kPencilCols;
+        const int ncol = min(kPencilCols, NK - kx0);
+        ok = htasync::bar_wait(&bar, parity);
+        if (__syncthreads_or(!ok)) {
+            ok = false;
+            break;
+        }
+        parity ^= 1;
+        htfft::C2 v[T];
+        if (w < ncol) {
+            const float2* col = in + w * N;
 #pragma unroll
-    for (int t = 0; t < TH; ++t) dst[lane + 32 * t] = col[htfft::lm_slot<TH>(lane + 32 * t)];
+            for (int t = 0; t < T; ++t) {
+                const float2 e = col[lane + 32 * t];
+                v[t] = {e.x, e.y};
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
+        if (w < ncol) {   // warp-uniform; no CTA barrier inside
+            htfft::warp_ifft_regs<T>(v, twL, lane, w32);
+            htfft::warp_ifft_store<T>(ob + w * S, v, lane);
+        }
+        __syncthreads();
+        pencil_store<T, S>(ob, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry, ncol, tid);
+    }
+    if (!ok && tid == 0) {
+        atomicExch(status, 1);
+        htasync::bar_wait(&bar, parity);
+    }
+}
+
+// TH = n / 64: the packed rows have M = n / 2 = 32 TH points.  Every warp streams rows
+// r = global warp, + total warps, ... through two slots: row r + stride is copied into the
+// other slot while row r is packed, transformed and stored.
+template <int TH>
+__global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
+                                                 float2* __restrict__ out, int NKP, int zlo,
+                                                 int ylo, int Ry, long long rows,
+                                                 const float2* __restrict__ twp,
+                                                 const float2* __restrict__ twM,
+                                                 const float2* __restrict__ tw32,
+                                                 int32_t* __restrict__ status) {
+    constexpr int M = 32 * TH, N = 2 * M, S = pencil_slot_x<TH>();
+    static_assert(S >= M + 2, "a padded C row must fit a slot");
+    extern __shared__ __align__(128) float2 sm[];
+    __shared__ __align__(8) unsigned long long bars[8][2];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    float2* slots = sm + w * 2 * S;
+    unsigned long long* bar = bars[w];
+    const long long stride = (long long)gridDim.x * 8;
+    const unsigned row_bytes = (unsigned)NKP * (unsigned)sizeof(float2);
+    long long r = (long long)blockIdx.x * 8 + w;
+    if (lane == 0) {
+        htasync::bar_init(&bar[0], 1);
+        htasync::bar_init(&bar[1], 1);
+        htasync::bar_init_fence();
+        if (r < rows) {
+            htasync::bar_expect(&bar[0], row_bytes);
+            htasync::bulk_load(slots, C + r * NKP, row_bytes, &bar[0]);
+        }
+    }
+    __syncwarp();
+    htfft::C2 w32[5];
+    htfft::lane_twiddles(lane, tw32, w32);
+    bool ok = true;
+    int i = 0;
+    for (; r < rows; ++i, r += stride) {
+        const int s = i & 1;
+        if (lane == 0 && r + stride < rows) {   // the other slot was released at the end of i - 1
+            htasync::fence_async_smem();
+            htasync::bar_expect(&bar[s ^ 1], row_bytes);
+            htasync::bulk_load(slots + (s ^ 1) * S, C + (r + stride) * NKP, row_bytes,
+                               &bar[s ^ 1]);
+        }
+        ok = htasync::bar_wait(&bar[s], (unsigned)((i >> 1) & 1));
+        if (__any_sync(0xffffffffu, !ok)) {
+            ok = false;
+            break;
+        }
+        float2* col = slots + s * S;
+        // half-length packing in place: lane handles the pair (k, M - k), k <= M / 2
+        for (int k = lane; k <= M / 2; k += 32) {
+            const float2 xa = col[k], xb = col[M - k];
+            auto pack = [&](float2 a, float2 bb, int kk) {
+                const float2 b = make_float2(bb.x, -bb.y);      // conj X[M - kk]
+                const float2 e = make_float2(a.x + b.x, a.y + b.y);
+                const float2 d = make_float2(a.x - b.x, a.y - b.y);
+                const float2 wv = __ldg(twp + kk);              // e^{2 pi i kk / N}
+                const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
+                return make_float2(e.x - o.y, e.y + o.x);
+            };
+            const float2 zk = pack(xa, xb, k);
+            const int kh = M - k;
+            if (kh != k && kh < M) col[kh] = pack(xb, xa, kh);
+            col[k] = zk;
+        }
+        __syncwarp();
+        htfft::C2 v[TH];
+#pragma unroll
+        for (int t = 0; t < TH; ++t) {
+            const float2 e = col[lane + 32 * t];
+            v[t] = {e.x, e.y};
+        }
+        htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
+        __syncwarp();
+        htfft::warp_ifft_store<TH>(col, v, lane);
+        __syncwarp();
+        const int zr = (int)(r / Ry), yr = (int)(r - (long long)zr * Ry);
+        float2* dst = out + ((long long)(zlo + zr) * N + (ylo + yr)) * M;
+#pragma unroll
+        for (int t = 0; t < TH; ++t) dst[lane + 32 * t] = col[htfft::lm_slot<TH>(lane + 32 * t)];
+        __syncwarp();
+    }
+    if (!ok && lane == 0) {
+        // record the timeout, then wait (bounded) for this warp's copies in flight
+        atomicExch(status, 1);
+        htasync::bar_wait(&bar[i & 1], (unsigned)((i >> 1) & 1));
+        if (r + stride < rows)
+            htasync::bar_wait(&bar[(i & 1) ^ 1], (unsigned)(((i + 1) >> 1) & 1));
+    }
 }
 
 }  // namespace
@@ -666,30 +853,38 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
 static bool pencil_side(int n) { return n == 576 || n == 1152; }
 
 // Z, Y and X passes from pencils P, through B and C (C may reuse P's buffer: P is read
-// only by the first pass).
+// only by the first pass).  Persistent grids: as many CTAs as fit on the device, capped by
+// the work items.
 template <int T>
 static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, float2* d_out,
                          int zlo, int zhi, int ylo, int yhi, cudaStream_t st) {
     constexpr int n = 32 * T, TH = T / 2;
-    const int nk = n / 2 + 1, Rz = zhi - zlo, Ry = yhi - ylo;
-    const size_t smyz = (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
-    const size_t smx = (size_t)8 * 33 * TH * sizeof(float2);
-    const float2* tw = (const float2*)ctx->d_ftw;
-    const float2* twL = tw;              // e^{2 pi i j / n}, j < n (also the packing twiddles)
-    const float2* twM = tw + n;          // e^{2 pi i j / (n/2)}
-    const float2* tw32 = tw + n + n / 2;
+    const int nk = n / 2 + 1, nkp = nk + 1, Rz = zhi - zlo, Ry = yhi - ylo;
+    const size_t smyz = pencil_smem_yz<T>(), smx = pencil_smem_x<TH>();
     HT_CUDA_TRY(cudaFuncSetAttribute(pz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "pz smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "py smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(px_kernel<TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "px smem");
-    pz_kernel<T><<<dim3((unsigned)(n / kPencilCols), (unsigned)nk), 256, smyz, st>>>(
-        P, B, nk, zlo, Rz, (const float*)ctx->d_win, twL, tw32);
-    HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
-    py_kernel<T><<<dim3((unsigned)((nk + kPencilCols - 1) / kPencilCols), (unsigned)Rz), 256,
-                   smyz, st>>>(B, C, nk, Rz, ylo, Ry, twL, tw32);
-    HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
+    int bz = 0, by = 0, bx = 0;
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bz, pz_kernel<T>, 256, smyz), "pz occupancy");
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, py_kernel<T>, 256, smyz), "py occupancy");
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bx, px_kernel<TH>, 256, smx), "px occupancy");
+    if (bz < 1 || by < 1 || bx < 1) return ht_fail(HT_ERR_CUDA, "pencil kernels do not fit an SM");
+    const FusedTw tw = fused_tw(ctx, n);
+    int32_t* status = ht_status_word(ctx);
+    const long long sms = ctx->num_sms;
+    const long long zt = (long long)nk * (n / kPencilCols);
+    const long long yt = (long long)Rz * ((nk + kPencilCols - 1) / kPencilCols);
     const long long rows = (long long)Rz * Ry;
-    px_kernel<TH><<<(unsigned)((rows + 7) / 8), 256, smx, st>>>(C, d_out, zlo, ylo, Ry, rows,
-                                                                twL, twM, tw32);
+    const unsigned gz = (unsigned)std::min(zt, sms * bz);
+    const unsigned gy = (unsigned)std::min(yt, sms * by);
+    const unsigned gx = (unsigned)std::min((rows + 7) / 8, sms * bx);
+    pz_kernel<T><<<gz, 256, smyz, st>>>(P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL,
+                                        tw.w32, status);
+    HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
+    py_kernel<T><<<gy, 256, smyz, st>>>(B, C, nk, nkp, Rz, ylo, Ry, tw.lmL, tw.w32, status);
+    HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
+    px_kernel<TH><<<gx, 256, smx, st>>>(C, d_out, nkp, zlo, ylo, Ry, rows, tw.nat, tw.lmM,
+                                        tw.w32, status);
     HT_CUDA_TRY(cudaGetLastError(), "px_kernel launch");
     return HT_OK;
 }
@@ -724,11 +919,15 @@ static int smooth_pencil_run(ht_ctx* ctx, const float2* P, float* d_out, int n, 
                              double Rf, int wsmooth, int zlo, int zhi, int ylo, int yhi,
                              cudaStream_t st) {
     const size_t nk = (size_t)n / 2 + 1;
+    const size_t cbytes = (nk + 1) * (size_t)(zhi - zlo) * (yhi - ylo) * sizeof(float2);
+    // C takes the first buffer; when P lives there too it must already be large enough
+    // (a reallocation here would free P before the first pass reads it)
+    if ((const void*)P == ctx->d_cwork && ctx->cwork_bytes < cbytes)
+        return ht_fail(HT_ERR_STATE, "smooth_pencil_run: pencil buffer smaller than C");
     int rc = ht_grow(&ctx->d_cwork2, &ctx->cwork2_bytes,
                      nk * (size_t)(zhi - zlo) * n * sizeof(float2), "smoothing buffer 2");
-    if (rc == HT_OK)
-        rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes,
-                     nk * (size_t)(zhi - zlo) * (yhi - ylo) * sizeof(float2), "smoothing buffer");
+    if (rc == HT_OK)   // C rows carry one pad element
+        rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
     if (rc == HT_OK) rc = fused_tables(ctx, n);
     if (rc == HT_OK) rc = scaled_window_table(ctx, n, boxsize, Rf, wsmooth, st);
     if (rc != HT_OK) return rc;
@@ -749,8 +948,11 @@ static int smooth_tile_pencil(ht_ctx* ctx, const void* d_delta_k, float* d_out, 
                               double boxsize, double Rf, int wsmooth, int zlo, int zhi,
                               cudaStream_t st) {
     const size_t nk = (size_t)n / 2 + 1;
-    int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, nk * n * n * sizeof(float2),
-                     "smoothing buffer");
+    // the buffer holds P, then C (rows of nk + 1 for z in [zlo, zhi), all y): size it for
+    // both before P is written
+    const size_t need = std::max(nk * n * n, (nk + 1) * (size_t)(zhi - zlo) * n) *
+                        sizeof(float2);
+    int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, need, "smoothing buffer");
     if (rc != HT_OK) return rc;
     float2* P = (float2*)ctx->d_cwork;
     rc = launch_pencil_transpose((const float2*)d_delta_k, P, n, st);
