@@ -28,6 +28,7 @@ __device__ __forceinline__ C2 mul(C2 a, C2 b) {
 }
 __device__ __forceinline__ C2 muli(C2 a) { return {-a.y, a.x}; }   // i * a
 __device__ __forceinline__ C2 scale(C2 a, float s) { return {a.x * s, a.y * s}; }
+__device__ __forceinline__ C2 to_c2(float2 e) { return {e.x, e.y}; }
 
 // e^{2 pi i j / N} for the small composite sizes used in registers (N = 9, 18, 36); this
 // header belongs to one translation unit (ht_smooth.cu), which fills them at set-up.
@@ -169,8 +170,7 @@ __device__ __forceinline__ void warp_ifft(float2* col, const float2* __restrict_
     C2 v[T];
 #pragma unroll
     for (int t = 0; t < T; ++t) {
-        const float2 e = col[lane + 32 * t];
-        v[t] = {e.x, e.y};
+        v[t] = to_c2(col[lane + 32 * t]);
     }
     warp_ifft_regs<T>(v, twLM, lane, w32);
     __syncwarp();

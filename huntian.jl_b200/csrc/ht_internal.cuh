@@ -45,7 +45,7 @@ struct ht_ctx {
     int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)
     int tune_walk_bpsm = 0;        // walk: blocks per SM (0: occupancy maximum)
     int tune_fft_path = 0;         // tile smoothing: 0 auto, 1 3-D plan, 2 transposed 1-D,
-                                   // 3 fused three-pass (n = 576, 1152)
+                                   // 3 fused three-pass, 4 pencil (n = 576, 1152)
 
     // collapse table + SPH table
     std::vector<float> h_ct;

@@ -549,12 +549,15 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
 // [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.  C rows carry one pad
 // element (n/2 + 2 complex values) so that every row starts on 16 bytes.
 //
-// All three kernels are persistent and software-pipelined: the next work item's columns
-// arrive by 1-D bulk copies (cp.async.bulk, completing on an mbarrier) while the current
-// one is transformed.  Z and Y: a CTA takes 8 neighbouring columns (8 warps, one column
-// each), reads them from shared memory into registers, issues the next item's copies,
-// transforms, and stores the 8 results through shared memory in 64-byte pieces of the
-// next layout.  X: every warp streams rows with a two-slot ring of its own.
+// All three kernels are persistent; columns and rows arrive by 1-D bulk copies
+// (cp.async.bulk, completing on an mbarrier that one thread polls with a bounded wait).
+// Z and Y: a CTA takes 8 neighbouring columns (8 warps, one column each), reads them from
+// its shared-memory slot into registers, transforms, writes the 8 results back into the
+// same slot in lane-major order and stores them in 64-byte pieces of the next layout, then
+// requests the next item's columns; two CTAs per SM overlap one's copies with the other's
+// arithmetic (measured faster than one CTA per SM with a second slot).  X: every warp
+// streams rows through a two-slot ring of its own, the next row in flight while the
+// current one is transformed.
 
 namespace {
 
@@ -566,10 +569,11 @@ __host__ __device__ constexpr int pencil_stride() {
     return 33 * T + (((2 - 33 * T) % 16) + 16) % 16;
 }
 
-// Z / Y shared memory: 8 input columns (bulk-copy destination) + 8 lane-major outputs
+// Z / Y shared memory: one slot of 8 columns, the bulk-copy destination (stride N) and
+// then the lane-major outputs (stride S >= N)
 template <int T>
 constexpr size_t pencil_smem_yz() {
-    return (size_t)kPencilCols * (32 * T + pencil_stride<T>()) * sizeof(float2);
+    return (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
 }
 
 // X: a warp's slot holds 33 TH complex values rounded up to even (16-byte slots; a padded
@@ -596,7 +600,7 @@ __device__ __forceinline__ void pencil_store(const float2* __restrict__ ob, floa
 }
 
 template <int T>
-__global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P,
+__global__ void __launch_bounds__(256, 2) pz_kernel(const float2* __restrict__ P,
                                                     float2* __restrict__ B, int NK, int zlo,
                                                     int Rz, const float* __restrict__ tab,
                                                     const float2* __restrict__ twL,
@@ -604,8 +608,8 @@ __global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P
                                                     int32_t* __restrict__ status) {
     constexpr int N = 32 * T, S = pencil_stride<T>(), NB = N / kPencilCols, H = T / 2;
     extern __shared__ __align__(128) float2 sm[];
-    float2* in = sm;                          // 8 columns of N
-    float2* ob = sm + kPencilCols * N;        // 8 lane-major columns of S
+    float2* in = sm;                          // 8 input columns of N
+    float2* ob = sm;                          // then 8 lane-major columns of S
     __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int ntasks = NK * NB;               // task = kx * NB + ky block
@@ -643,7 +647,7 @@ __global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P
             wl[t] = __ldg(tab + (base + kz * kz));
         }
         const float wmid = __ldg(tab + (base + (N / 2) * (N / 2)));
-        ok = htasync::bar_wait(&bar, parity);
+        ok = tid == 0 ? htasync::bar_wait(&bar, parity) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
             break;
@@ -653,14 +657,9 @@ __global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P
         const float2* col = in + w * N;
 #pragma unroll
         for (int t = 0; t < T; ++t) {
-            const float2 e = col[lane + 32 * t];
-            v[t] = {e.x, e.y};
+            v[t] = htfft::to_c2(col[lane + 32 * t]);
         }
-        __syncthreads();                      // every column is in registers: refill `in`
-        if (tid == 0 && task + (int)gridDim.x < ntasks) {
-            htasync::fence_async_smem();
-            issue(task + (int)gridDim.x);
-        }
+        __syncthreads();                      // every column is in registers: reuse the slot
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             float wv;
@@ -678,6 +677,11 @@ __global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P
         htfft::warp_ifft_store<T>(ob + w * S, v, lane);
         __syncthreads();
         pencil_store<T, S>(ob, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, kPencilCols, tid);
+        __syncthreads();
+        if (tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
     }
     if (!ok && tid == 0) {
         // record the timeout, then wait (bounded) for the copy still in flight
@@ -687,7 +691,7 @@ __global__ void __launch_bounds__(256, 1) pz_kernel(const float2* __restrict__ P
 }
 
 template <int T>
-__global__ void __launch_bounds__(256, 1) py_kernel(const float2* __restrict__ B,
+__global__ void __launch_bounds__(256, 2) py_kernel(const float2* __restrict__ B,
                                                     float2* __restrict__ C, int NK, int NKP,
                                                     int Rz, int ylo, int Ry,
                                                     const float2* __restrict__ twL,
@@ -696,7 +700,7 @@ __global__ void __launch_bounds__(256, 1) py_kernel(const float2* __restrict__ B
     constexpr int N = 32 * T, S = pencil_stride<T>();
     extern __shared__ __align__(128) float2 sm[];
     float2* in = sm;
-    float2* ob = sm + kPencilCols * N;
+    float2* ob = sm;
     __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int NKB = (NK + kPencilCols - 1) / kPencilCols;
@@ -723,7 +727,7 @@ __global__ void __launch_bounds__(256, 1) py_kernel(const float2* __restrict__ B
     for (; task < ntasks; task += gridDim.x) {
         const int zr = task / NKB, kx0 = (task - zr * NKB) * kPencilCols;
         const int ncol = min(kPencilCols, NK - kx0);
-        ok = htasync::bar_wait(&bar, parity);
+        ok = tid == 0 ? htasync::bar_wait(&bar, parity) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
             break;
@@ -734,21 +738,21 @@ __global__ void __launch_bounds__(256, 1) py_kernel(const float2* __restrict__ B
             const float2* col = in + w * N;
 #pragma unroll
             for (int t = 0; t < T; ++t) {
-                const float2 e = col[lane + 32 * t];
-                v[t] = {e.x, e.y};
+                v[t] = htfft::to_c2(col[lane + 32 * t]);
             }
         }
         __syncthreads();
-        if (tid == 0 && task + (int)gridDim.x < ntasks) {
-            htasync::fence_async_smem();
-            issue(task + (int)gridDim.x);
-        }
         if (w < ncol) {   // warp-uniform; no CTA barrier inside
             htfft::warp_ifft_regs<T>(v, twL, lane, w32);
             htfft::warp_ifft_store<T>(ob + w * S, v, lane);
         }
         __syncthreads();
         pencil_store<T, S>(ob, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry, ncol, tid);
+        __syncthreads();
+        if (tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
     }
     if (!ok && tid == 0) {
         atomicExch(status, 1);
@@ -799,7 +803,8 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
             htasync::bulk_load(slots + (s ^ 1) * S, C + (r + stride) * NKP, row_bytes,
                                &bar[s ^ 1]);
         }
-        ok = htasync::bar_wait(&bar[s], (unsigned)((i >> 1) & 1));
+        ok = lane == 0 ? htasync::bar_wait(&bar[s], (unsigned)((i >> 1) & 1)) : true;
+        __syncwarp();
         if (__any_sync(0xffffffffu, !ok)) {
             ok = false;
             break;
@@ -825,8 +830,7 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
         htfft::C2 v[TH];
 #pragma unroll
         for (int t = 0; t < TH; ++t) {
-            const float2 e = col[lane + 32 * t];
-            v[t] = {e.x, e.y};
+            v[t] = htfft::to_c2(col[lane + 32 * t]);
         }
         htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
         __syncwarp();
