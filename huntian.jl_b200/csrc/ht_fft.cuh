@@ -30,14 +30,20 @@ __device__ __forceinline__ C2 muli(C2 a) { return {-a.y, a.x}; }   // i * a
 __device__ __forceinline__ C2 scale(C2 a, float s) { return {a.x * s, a.y * s}; }
 __device__ __forceinline__ C2 to_c2(float2 e) { return {e.x, e.y}; }
 
-// e^{2 pi i j / N} for the small composite sizes used in registers (N = 9, 18, 36); this
-// header belongs to one translation unit (ht_smooth.cu), which fills them at set-up.
+// e^{2 pi i j / N} for the small composite sizes used in registers (N = 8, 9, 18, 32, 36);
+// this header belongs to one translation unit (ht_smooth.cu), which fills them at set-up.
+__constant__ float2 c_w8[8];
 __constant__ float2 c_w9[9];
 __constant__ float2 c_w18[18];
+__constant__ float2 c_w32[32];
 __constant__ float2 c_w36[36];
 
 template <int N>
 __device__ __forceinline__ C2 wsmall(int j);   // e^{2 pi i j / N}, j in [0, N)
+template <>
+__device__ __forceinline__ C2 wsmall<8>(int j) { const float2 w = c_w8[j]; return {w.x, w.y}; }
+template <>
+__device__ __forceinline__ C2 wsmall<32>(int j) { const float2 w = c_w32[j]; return {w.x, w.y}; }
 template <>
 __device__ __forceinline__ C2 wsmall<9>(int j) { const float2 w = c_w9[j]; return {w.x, w.y}; }
 template <>
@@ -83,6 +89,16 @@ struct Dft<4> {
     }
 };
 
+// a e^{2 pi i j / N}; the quarter turns (j N/4) are sign changes and swaps
+template <int N>
+__device__ __forceinline__ C2 twiddle(C2 a, int j) {
+    if (j == 0) return a;
+    if (4 * j == N) return muli(a);
+    if (2 * j == N) return {-a.x, -a.y};
+    if (4 * j == 3 * N) return {a.y, -a.x};
+    return mul(a, wsmall<N>(j));
+}
+
 // N = R1 R2: x[t1 + R1 t2] -> y[k2 + R2 k1] = sum_t1 w_R1^{t1 k1} w_N^{t1 k2}
 //                                               sum_t2 x[t1 + R1 t2] w_R2^{t2 k2}
 template <int R1, int R2>
@@ -98,7 +114,7 @@ struct DftComposite {
             Dft<R2>::run(a);
 #pragma unroll
             for (int k2 = 0; k2 < R2; ++k2)
-                u[t1 + R1 * k2] = (t1 * k2) % N == 0 ? a[k2] : mul(a[k2], wsmall<N>((t1 * k2) % N));
+                u[t1 + R1 * k2] = twiddle<N>(a[k2], (t1 * k2) % N);
         }
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
@@ -112,6 +128,14 @@ struct DftComposite {
     }
 };
 
+template <>
+struct Dft<8> {
+    __device__ __forceinline__ static void run(C2 (&v)[8]) { DftComposite<2, 4>::run(v); }
+};
+template <>
+struct Dft<32> {
+    __device__ __forceinline__ static void run(C2 (&v)[32]) { DftComposite<4, 8>::run(v); }
+};
 template <>
 struct Dft<9> {
     __device__ __forceinline__ static void run(C2 (&v)[9]) { DftComposite<3, 3>::run(v); }
@@ -127,6 +151,66 @@ struct Dft<36> {
 
 __device__ __forceinline__ int bitrev5(int l) { return __brev((unsigned)l) >> 27; }
 
+// Shared-memory slot of y[i] in the "row-major" column layout of the transposed form:
+// row k2 = i mod T holds y[k2 + T k1] at k2 * 33 + k1 (32 values and a pad), so that a
+// warp writing X[lane][k2] for one k2 covers 32 consecutive slots and a thread reading
+// row k2 walks consecutive slots.  A column needs 33 T slots.
+template <int T>
+__device__ __forceinline__ int km_slot(int i) {
+    const int k1 = i / T;
+    return (i - T * k1) * 33 + k1;
+}
+
+// The 32-point DFT of row k2 of a row-major column (in place): x[l] = X[l][k2] at
+// k2 * 33 + l on entry, y[k2 + T k1] at k2 * 33 + k1 on exit.
+__device__ __forceinline__ void dft32_row(float2* row) {
+    C2 v[32];
+#pragma unroll
+    for (int l = 0; l < 32; ++l) v[l] = to_c2(row[l]);
+    Dft<32>::run(v);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) row[k] = make_float2(v[k].x, v[k].y);
+}
+
+// Steps 1-2 only: on entry lane holds v[t] = x[lane + 32 t]; on exit v[k2] is the twiddled
+// inner transform X[lane][k2], whose 32-point DFTs over the lanes (one per k2) give
+// y[k2 + T k1].  For kernels that finish those DFTs in registers after a shared-memory
+// transpose (dft32_rows) instead of across lanes.
+template <int T>
+__device__ __forceinline__ void warp_ifft_inner(C2 (&v)[T], const float2* __restrict__ twLM,
+                                                int lane) {
+    Dft<T>::run(v);
+#pragma unroll
+    for (int k2 = 1; k2 < T; ++k2) {
+        const float2 w = __ldg(twLM + 32 * k2 + lane);
+        v[k2] = mul(v[k2], {w.x, w.y});
+    }
+}
+
+// Step 3 for rows k2 in [K0, T): the 32-point DFT across lanes, decimation in frequency
+// (spans 16, 8, 4, 2, 1); lane l ends with y[k2 + T k1], k1 = bitrev5(l).  Lower lane:
+// a + b; upper lane: (b - a) w_{2s}^{lane mod s}, written as one signed sum b + sg a and a
+// product by we (1 on lower lanes, and on every lane of the last stage, where w_2^0 = 1):
+// the same roundings as the two-branch form, a third of the work.
+template <int T, int K0>
+__device__ __forceinline__ void cross32(C2 (&v)[T], int lane, const C2 (&w32)[5]) {
+#pragma unroll
+    for (int st = 4; st >= 0; --st) {
+        const int s = 1 << st;
+        const bool upper = (lane & s) != 0;
+        const float sg = upper ? -1.f : 1.f;
+        const C2 we = upper ? w32[st] : C2{1.f, 0.f};
+#pragma unroll
+        for (int k2 = K0; k2 < T; ++k2) {
+            const C2 a = v[k2];
+            const C2 b = {__shfl_xor_sync(0xffffffffu, a.x, s),
+                          __shfl_xor_sync(0xffffffffu, a.y, s)};
+            const C2 r = {fmaf(sg, a.x, b.x), fmaf(sg, a.y, b.y)};
+            v[k2] = st == 0 ? r : mul(r, we);
+        }
+    }
+}
+
 // Steps 1-3 on registers: on entry lane holds v[t] = x[lane + 32 t]; on exit v[k2] =
 // y[k2 + T k1] with k1 = bitrev5(lane).
 // twLM[32 k2 + l] = e^{2 pi i l k2 / (32 T)}, k2 < T, l < 32 (global, cached).  w32[s] for
@@ -135,31 +219,8 @@ __device__ __forceinline__ int bitrev5(int l) { return __brev((unsigned)l) >> 27
 template <int T>
 __device__ __forceinline__ void warp_ifft_regs(C2 (&v)[T], const float2* __restrict__ twLM,
                                                int lane, const C2 (&w32)[5]) {
-    Dft<T>::run(v);
-#pragma unroll
-    for (int k2 = 1; k2 < T; ++k2) {
-        const float2 w = __ldg(twLM + 32 * k2 + lane);
-        v[k2] = mul(v[k2], {w.x, w.y});
-    }
-    // 32-point DFT across lanes, decimation in frequency: spans 16, 8, 4, 2, 1
-#pragma unroll
-    // Lower lane: a + b; upper lane: (b - a) w_{2s}^{lane mod s}, written as one signed sum
-    // b + sg a and a product by we (1 on lower lanes, and on every lane of the last stage,
-    // where w_2^0 = 1): the same roundings as the two-branch form, a third of the work.
-    for (int st = 4; st >= 0; --st) {
-        const int s = 1 << st;
-        const bool upper = (lane & s) != 0;
-        const float sg = upper ? -1.f : 1.f;
-        const C2 we = upper ? w32[st] : C2{1.f, 0.f};
-#pragma unroll
-        for (int k2 = 0; k2 < T; ++k2) {
-            const C2 a = v[k2];
-            const C2 b = {__shfl_xor_sync(0xffffffffu, a.x, s),
-                          __shfl_xor_sync(0xffffffffu, a.y, s)};
-            const C2 r = {fmaf(sg, a.x, b.x), fmaf(sg, a.y, b.y)};
-            v[k2] = st == 0 ? r : mul(r, we);
-        }
-    }
+    warp_ifft_inner<T>(v, twLM, lane);
+    cross32<T, 0>(v, lane, w32);
 }
 
 // Inverse FFT of the column col[0 .. 32 T) (shared memory, float2), in place, natural

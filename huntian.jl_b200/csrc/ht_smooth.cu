@@ -473,10 +473,14 @@ static int fused_tables(ht_ctx* ctx, int n) {
     if (rc != HT_OK) return rc;
     HT_CUDA_TRY(cudaMemcpy(ctx->d_ftw, t.data(), t.size() * sizeof(float2), cudaMemcpyHostToDevice),
                 "twiddle upload");
-    float2 c9[9], c18[18], c36[36];
+    float2 c8[8], c9[9], c18[18], c32[32], c36[36];
+    for (int j = 0; j < 8; ++j) c8[j] = w(j, 8);
     for (int j = 0; j < 9; ++j) c9[j] = w(j, 9);
     for (int j = 0; j < 18; ++j) c18[j] = w(j, 18);
+    for (int j = 0; j < 32; ++j) c32[j] = w(j, 32);
     for (int j = 0; j < 36; ++j) c36[j] = w(j, 36);
+    HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w8, c8, sizeof c8), "c_w8");
+    HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w32, c32, sizeof c32), "c_w32");
     HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w9, c9, sizeof c9), "c_w9");
     HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w18, c18, sizeof c18), "c_w18");
     HT_CUDA_TRY(cudaMemcpyToSymbol(htfft::c_w36, c36, sizeof c36), "c_w36");
@@ -563,14 +567,14 @@ namespace {
 
 constexpr int kPencilCols = 8;   // columns (warps) per CTA in the Z and Y passes
 
-// lane-major column of 33 T slots, padded so that 8 columns start 2 banks apart
+// row-major column of 33 T slots (km_slot), padded so that 8 columns start 2 banks apart
 template <int T>
 __host__ __device__ constexpr int pencil_stride() {
     return 33 * T + (((2 - 33 * T) % 16) + 16) % 16;
 }
 
 // Z / Y shared memory: one slot of 8 columns, the bulk-copy destination (stride N) and
-// then the lane-major outputs (stride S >= N)
+// then the row-major outputs (stride S >= N)
 template <int T>
 constexpr size_t pencil_smem_yz() {
     return (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
@@ -587,29 +591,54 @@ constexpr size_t pencil_smem_x() {
     return (size_t)8 * 2 * pencil_slot_x<TH>() * sizeof(float2);
 }
 
-// Transposed store of the CTA's 8 lane-major columns: dst[r * pitch + c] = column c's
-// output lo + r, for r < R and c < ncol.
+// Rows of the 32-point DFTs finished in registers after the transpose: up to 32 per
+// column, so that 8 columns give at most one per thread; rows beyond (T > 32) are finished
+// across the lanes in the warp.
+template <int T>
+__host__ __device__ constexpr int pencil_rows() {
+    return T < 32 ? T : 32;
+}
+
+// The second half of the Z / Y transforms and the transposed store.  On entry warp w < ncol
+// holds its column's twiddled inner transform X[lane][k2] in registers, rows k2 >=
+// pencil_rows already finished across lanes (y[k2 + T bitrev5(lane)]): it writes every row
+// k2 to slots k2 * 33 + (lane or k1), the CTA finishes the remaining 32-point row DFTs one
+// per thread, and dst[r * pitch + c] = column c's output lo + r for r < R, c < ncol.
 template <int T, int S>
-__device__ __forceinline__ void pencil_store(const float2* __restrict__ ob, float2* dst,
-                                             long long pitch, int lo, int R, int ncol,
-                                             int tid) {
+__device__ __forceinline__ void pencil_finish(float2* __restrict__ ob,
+                                              const htfft::C2 (&v)[T], float2* dst,
+                                              long long pitch, int lo, int R, int ncol,
+                                              int tid) {
+    constexpr int TB = pencil_rows<T>();
+    const int lane = tid & 31, w = tid >> 5;
+    if (w < ncol) {
+#pragma unroll
+        for (int k2 = 0; k2 < TB; ++k2) ob[w * S + k2 * 33 + lane] = make_float2(v[k2].x, v[k2].y);
+        const int k1 = htfft::bitrev5(lane);
+#pragma unroll
+        for (int k2 = TB; k2 < T; ++k2) ob[w * S + k2 * 33 + k1] = make_float2(v[k2].x, v[k2].y);
+    }
+    __syncthreads();
+    for (int j = tid; j < ncol * TB; j += 256) {
+        const int c = j / TB, k2 = j - c * TB;
+        htfft::dft32_row(ob + c * S + k2 * 33);
+    }
+    __syncthreads();
     for (int e = tid; e < kPencilCols * R; e += 256) {
         const int r = e >> 3, c = e & 7;
-        if (c < ncol) dst[(long long)r * pitch + c] = ob[c * S + htfft::lm_slot<T>(lo + r)];
+        if (c < ncol) dst[(long long)r * pitch + c] = ob[c * S + htfft::km_slot<T>(lo + r)];
     }
 }
 
 template <int T>
-__global__ void __launch_bounds__(256, 2) pz_kernel(const float2* __restrict__ P,
-                                                    float2* __restrict__ B, int NK, int zlo,
-                                                    int Rz, const float* __restrict__ tab,
-                                                    const float2* __restrict__ twL,
-                                                    const float2* __restrict__ tw32,
-                                                    int32_t* __restrict__ status) {
+__global__ void __launch_bounds__(256, 2) pz_kernel(
+    const float2* __restrict__ P, float2* __restrict__ B, int NK, int zlo, int Rz,
+    const float* __restrict__ tab, const float2* __restrict__ twL,
+    const float2* __restrict__ tw32, int32_t* __restrict__ status) {
     constexpr int N = 32 * T, S = pencil_stride<T>(), NB = N / kPencilCols, H = T / 2;
     extern __shared__ __align__(128) float2 sm[];
     float2* in = sm;                          // 8 input columns of N
-    float2* ob = sm;                          // then 8 lane-major columns of S
+    float2* ob = sm;                          // then 8 row-major columns of S
     __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int ntasks = NK * NB;               // task = kx * NB + ky block
@@ -656,9 +685,7 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(const float2* __restrict__ P
         htfft::C2 v[T];
         const float2* col = in + w * N;
 #pragma unroll
-        for (int t = 0; t < T; ++t) {
-            v[t] = htfft::to_c2(col[lane + 32 * t]);
-        }
+        for (int t = 0; t < T; ++t) v[t] = htfft::to_c2(col[lane + 32 * t]);
         __syncthreads();                      // every column is in registers: reuse the slot
 #pragma unroll
         for (int t = 0; t < T; ++t) {
@@ -673,10 +700,10 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(const float2* __restrict__ P
             v[t].x *= wv;
             v[t].y *= wv;
         }
-        htfft::warp_ifft_regs<T>(v, twL, lane, w32);
-        htfft::warp_ifft_store<T>(ob + w * S, v, lane);
-        __syncthreads();
-        pencil_store<T, S>(ob, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, kPencilCols, tid);
+        htfft::warp_ifft_inner<T>(v, twL, lane);
+        htfft::cross32<T, pencil_rows<T>()>(v, lane, w32);
+        pencil_finish<T, S>(ob, v, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, kPencilCols,
+                            tid);
         __syncthreads();
         if (tid == 0 && task + (int)gridDim.x < ntasks) {
             htasync::fence_async_smem();
@@ -691,12 +718,10 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(const float2* __restrict__ P
 }
 
 template <int T>
-__global__ void __launch_bounds__(256, 2) py_kernel(const float2* __restrict__ B,
-                                                    float2* __restrict__ C, int NK, int NKP,
-                                                    int Rz, int ylo, int Ry,
-                                                    const float2* __restrict__ twL,
-                                                    const float2* __restrict__ tw32,
-                                                    int32_t* __restrict__ status) {
+__global__ void __launch_bounds__(256, 2) py_kernel(
+    const float2* __restrict__ B, float2* __restrict__ C, int NK, int NKP, int Rz, int ylo,
+    int Ry, const float2* __restrict__ twL, const float2* __restrict__ tw32,
+    int32_t* __restrict__ status) {
     constexpr int N = 32 * T, S = pencil_stride<T>();
     extern __shared__ __align__(128) float2 sm[];
     float2* in = sm;
@@ -737,17 +762,14 @@ __global__ void __launch_bounds__(256, 2) py_kernel(const float2* __restrict__ B
         if (w < ncol) {
             const float2* col = in + w * N;
 #pragma unroll
-            for (int t = 0; t < T; ++t) {
-                v[t] = htfft::to_c2(col[lane + 32 * t]);
-            }
+            for (int t = 0; t < T; ++t) v[t] = htfft::to_c2(col[lane + 32 * t]);
         }
         __syncthreads();
-        if (w < ncol) {   // warp-uniform; no CTA barrier inside
-            htfft::warp_ifft_regs<T>(v, twL, lane, w32);
-            htfft::warp_ifft_store<T>(ob + w * S, v, lane);
+        if (w < ncol) {   // warp-uniform
+            htfft::warp_ifft_inner<T>(v, twL, lane);
+            htfft::cross32<T, pencil_rows<T>()>(v, lane, w32);
         }
-        __syncthreads();
-        pencil_store<T, S>(ob, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry, ncol, tid);
+        pencil_finish<T, S>(ob, v, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry, ncol, tid);
         __syncthreads();
         if (tid == 0 && task + (int)gridDim.x < ntasks) {
             htasync::fence_async_smem();
@@ -869,8 +891,9 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
     HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "py smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(px_kernel<TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "px smem");
     int bz = 0, by = 0, bx = 0;
-    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bz, pz_kernel<T>, 256, smyz), "pz occupancy");
-    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, py_kernel<T>, 256, smyz), "py occupancy");
+    constexpr int nty = 256;
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bz, pz_kernel<T>, nty, smyz), "pz occupancy");
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, py_kernel<T>, nty, smyz), "py occupancy");
     HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bx, px_kernel<TH>, 256, smx), "px occupancy");
     if (bz < 1 || by < 1 || bx < 1) return ht_fail(HT_ERR_CUDA, "pencil kernels do not fit an SM");
     const FusedTw tw = fused_tw(ctx, n);
@@ -882,10 +905,10 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
     const unsigned gz = (unsigned)std::min(zt, sms * bz);
     const unsigned gy = (unsigned)std::min(yt, sms * by);
     const unsigned gx = (unsigned)std::min((rows + 7) / 8, sms * bx);
-    pz_kernel<T><<<gz, 256, smyz, st>>>(P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL,
+    pz_kernel<T><<<gz, nty, smyz, st>>>(P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL,
                                         tw.w32, status);
     HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
-    py_kernel<T><<<gy, 256, smyz, st>>>(B, C, nk, nkp, Rz, ylo, Ry, tw.lmL, tw.w32, status);
+    py_kernel<T><<<gy, nty, smyz, st>>>(B, C, nk, nkp, Rz, ylo, Ry, tw.lmL, tw.w32, status);
     HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
     px_kernel<TH><<<gx, 256, smx, st>>>(C, d_out, nkp, zlo, ylo, Ry, rows, tw.nat, tw.lmM,
                                         tw.w32, status);
