@@ -29,7 +29,11 @@ import tempfile
 import time
 
 import numpy as np
-import torch
+
+# tile1152 keeps ~150 GB resident (fields, cell records, spectrum, smoothing buffers): let
+# the caching allocator grow segments instead of fragmenting across the per-step temporaries
+os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+import torch  # noqa: E402
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
@@ -408,9 +412,12 @@ def run_ours(args, rank, world, device):
                      "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
                      "peak_source": peak_kind, "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes, "cells_walked": cells},
-        # ours per step: 2 window + 4 peak-scan kernels per filter, pack, order keys, walk
-        # (+ features and MLP in learned mode); cuFFT and CUB launches not counted
-        "gpu_launches": int(args.steps * (6 * nf + 3 + (2 if args.mode == "learned" else 0))),
+        # ours per step: per filter the window table + 3 transform kernels (pencil passes,
+        # or the transposed path's window/transpose kernels) and 4 peak-scan kernels; per
+        # step the pencil transpose, pack, order keys, walk (+ features and MLP in learned
+        # mode); cuFFT and CUB launches not counted
+        "gpu_launches": int(args.steps * (8 * nf + (1 if W.pencil else 0) + 3 +
+                                          (2 if args.mode == "learned" else 0))),
         "clocks": ck,
         "e2e": e2e,
     }
@@ -433,6 +440,7 @@ def run_e2e(ht, W, args):
     tot = 0
     for _ in range(args.e2e_steps):
         for k, v in host.items():
+            W.tile[k] = None                  # release the old copy before the new one
             W.tile[k] = v.to(W.device, non_blocking=True)
         npk = W.step()
         tot += npk

@@ -1,10 +1,12 @@
 """Build recipe for libhuntian_b200.so (sm_100a), in-tree next to this file.
 
-    python huntian.jl_b200/build.py [--verbose]
+    python huntian.jl_b200/build.py [--verbose] [--smallcase]
 
 Compiles every .cu under csrc/ with nvcc for sm_100a only (no fast-math: the collapse
 criterion needs IEEE divisions, square roots and NaN propagation) and links them into
-one shared library with a plain C ABI (include/huntian_b200.h).
+one shared library with a plain C ABI (include/huntian_b200.h).  --smallcase also builds
+pencil_smallcase, the reduced-size driver of the 1152^3 pencil smoothing kernels used for
+ncu captures.
 """
 import glob
 import os
@@ -43,6 +45,19 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+def build_smallcase() -> str:
+    """pencil_smallcase: pencil_smallcase.cu (which includes csrc/ht_smooth.cu) linked with
+    the other sources."""
+    out = os.path.join(HERE, "pencil_smallcase")
+    srcs = [os.path.join(HERE, "pencil_smallcase.cu")] + \
+        [f for f in sources() if os.path.basename(f) != "ht_smooth.cu"]
+    flags = [f for f in FLAGS if f not in ("-shared", "-Xcompiler", "-fPIC", "-fvisibility=hidden")]
+    subprocess.run([NVCC] + flags + ["-lcuda"] + srcs + ["-o", out], check=True)
+    return out
+
+
 if __name__ == "__main__":
     build(force=True, verbose="--verbose" in sys.argv)
     print(LIB)
+    if "--smallcase" in sys.argv:
+        print(build_smallcase())
