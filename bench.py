@@ -237,8 +237,10 @@ class Workload:
             self.pf_loop()
         torch.cuda.synchronize()
 
-    def step(self, ev=None):
-        """One tile: peak scan over all filters, then pack + shell collapse."""
+    def step(self, ev=None, fields_ready=None):
+        """One tile: peak scan over all filters, then pack + shell collapse.  fields_ready:
+        an event after which the six displacement fields are on the device (they are first
+        read by the pack, so their host copies may overlap the peak finding)."""
         import torch
         self.mask.zero_()
         self.peaks["count"].zero_()
@@ -264,6 +266,8 @@ class Workload:
         t = self.tile
         if ev is not None:
             ev["pack"][0].record()
+        if fields_ready is not None:
+            torch.cuda.current_stream().wait_event(fields_ready)
         self.finder.bind_fields(t["delta"], t["etax"], t["etay"], t["etaz"], t["eta2x"],
                                 t["eta2y"], t["eta2z"], None)
         if ev is not None:
@@ -426,33 +430,70 @@ def run_ours(args, rank, world, device):
 
 
 def run_e2e(ht, W, args):
-    """Same step through the public host-buffer API: fields start in pinned host memory,
-    are copied to the device inside the timed region, and all results (peaks, the 14
-    result arrays and the mask) are read back."""
+    """Same step through the public host-buffer API: fields start in pinned host memory and
+    are copied into the device tile inside the timed region, and all results (peaks, the 14
+    result arrays and the mask) are read back into pinned host buffers.  delta is copied
+    first; the six displacement fields, first needed by the pack, copy on a second stream
+    while the peak finding runs."""
     import torch
     host = {k: v.cpu().pin_memory() for k, v in W.tile.items()}
     h2d = sum(t.numel() * t.element_size() for t in host.values())
+    names = [("peaks", c) for c in ("i", "j", "k", "delta", "filter_idx")] + \
+        [("results", n) for n in ht.RESULT_NAMES]
+
+    def out_count(grp, n, npk):
+        return npk * (ht.RESULT_WIDTH.get(n, 1) if grp == "results" else 1)
+
+    out_host = {n: torch.empty(out_count(g, n, W.npeaks), dtype=getattr(W, g)[n].dtype)
+                .pin_memory() for g, n in names}
+    out_host["mask"] = torch.empty(W.mask.shape, dtype=W.mask.dtype).pin_memory()
+    side = torch.cuda.Stream()
+    main = torch.cuda.current_stream()
     d2h = 0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mk = lambda: torch.cuda.Event(enable_timing=True)
+    s0, s1 = mk(), mk()
+    parts = {"h2d_delta": 0.0, "step": 0.0, "d2h": 0.0}
     s0.record()
     tot = 0
     for _ in range(args.e2e_steps):
-        for k, v in host.items():
-            W.tile[k] = None                  # release the old copy before the new one
-            W.tile[k] = v.to(W.device, non_blocking=True)
-        npk = W.step()
+        e = [mk() for _ in range(4)]
+        e[0].record()
+        W.tile["delta"].copy_(host["delta"], non_blocking=True)   # into the device tile
+        e[1].record()
+        side.wait_stream(main)
+        with torch.cuda.stream(side):
+            for k, v in host.items():
+                if k != "delta":
+                    W.tile[k].copy_(v, non_blocking=True)
+            ready = torch.cuda.Event()
+            ready.record(side)
+        npk = W.step(fields_ready=ready)
         tot += npk
-        outs = [W.peaks[c][:npk].cpu() for c in ("i", "j", "k", "delta", "filter_idx")]
-        outs += [W.results[n][:npk * ht.RESULT_WIDTH.get(n, 1)].cpu() for n in ht.RESULT_NAMES]
-        outs.append(W.mask.cpu())
-        d2h = sum(o.numel() * o.element_size() for o in outs)
+        e[2].record()
+        d2h = 0
+        for grp, n in names:
+            src = getattr(W, grp)[n]
+            cnt = out_count(grp, n, npk)
+            if out_host[n].numel() < cnt:     # more peaks than the warm-up step found
+                out_host[n] = torch.empty(cnt, dtype=src.dtype).pin_memory()
+            out_host[n][:cnt].copy_(src[:cnt], non_blocking=True)
+            d2h += cnt * src.element_size()
+        out_host["mask"].copy_(W.mask, non_blocking=True)
+        d2h += W.mask.numel() * W.mask.element_size()
+        e[3].record()
+        torch.cuda.synchronize()
+        parts["h2d_delta"] += e[0].elapsed_time(e[1])
+        parts["step"] += e[1].elapsed_time(e[2])
+        parts["d2h"] += e[2].elapsed_time(e[3])
     s1.record()
     torch.cuda.synchronize()
     ms = s0.elapsed_time(s1)
+    k = max(1, args.e2e_steps)
     return {"value": tot / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms / args.e2e_steps,
+            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms / k,
+            "parts_ms": {p: v / k for p, v in parts.items()},
             "wall_s": time.perf_counter() - t0}
 
 
