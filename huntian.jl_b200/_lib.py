@@ -41,7 +41,8 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_fields_pack",
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
            "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
-           "ht_bracket_adam", "ht_ctx_tune")
+           "ht_bracket_adam", "ht_ctx_tune", "ht_ctx_set_cosmo", "ht_peak_lightcone",
+           "ht_pack_halos")
 
 
 class HTError(RuntimeError):
@@ -83,6 +84,23 @@ DIAG_NAMES = ("walk_shells", "collapse_shell")
 
 class HtResults(C.Structure):
     _fields_ = [(n, _P) for n in RESULT_NAMES] + [(n, _P) for n in DIAG_NAMES]
+
+
+class HtCosmo(C.Structure):
+    _fields_ = [("chi", _P), ("zchi", _P), ("n_chi", C.c_int32), ("z_max", C.c_double),
+                ("atab", _P), ("D_atab", _P), ("dlnD_dlna", _P), ("ntab", C.c_int32)] + \
+        [(n, C.c_double) for n in ("amintab", "amaxtab", "D_ainfty", "D_a0", "HD_Hainfty",
+                                   "HD_Ha0", "Om", "OL")]
+
+
+class HtTileGeom(C.Structure):
+    _fields_ = [("n", C.c_int32), ("xbx", C.c_double), ("ybx", C.c_double),
+                ("zbx", C.c_double), ("alatt", C.c_double)]
+
+
+class HtCatalogPeaks(C.Structure):
+    _fields_ = [(n, _P) for n in ("i", "j", "k", "Rf", "FcRf", "d2Rf", "z")] + \
+        [("npeaks", C.c_int64)]
 
 
 class HtBracketModel(C.Structure):
@@ -157,6 +175,14 @@ def load() -> C.CDLL:
     L.ht_bracket_adam.restype = C.c_int
     L.ht_bracket_adam.argtypes = [_P, _P, _P, _P, _P, i32, C.c_float,
                                   C.POINTER(HtBracketModel), _P]
+    L.ht_ctx_set_cosmo.restype = C.c_int
+    L.ht_ctx_set_cosmo.argtypes = [_P, C.POINTER(HtCosmo)]
+    L.ht_peak_lightcone.restype = C.c_int
+    L.ht_peak_lightcone.argtypes = [_P, _P, _P, _P, i64, C.POINTER(HtTileGeom), _P, dbl, _P,
+                                    _P, _P, _P, _P, _P]
+    L.ht_pack_halos.restype = C.c_int
+    L.ht_pack_halos.argtypes = [_P, C.POINTER(HtCatalogPeaks), C.POINTER(HtResults),
+                                C.POINTER(HtTileGeom), dbl, dbl, i32, i32, _P, i64, _P, _P]
     _lib = L
     return L
 

@@ -89,6 +89,20 @@ struct ht_ctx {
     size_t order_ws_bytes = 0;
     void* d_mlp_ws = nullptr;      // bracket training activations
     size_t mlp_ws_bytes = 0;
+    // lightcone and halo-record tables (ht_ctx_set_cosmo) and their workspace
+    bool cosmo_set = false;
+    double* d_chi = nullptr;       // chi -> z table
+    double* d_zchi = nullptr;
+    int n_chi = 0;
+    double cosmo_zmax = 0.0;
+    double* d_atab = nullptr;      // linear-growth tables
+    double* d_Da = nullptr;
+    double* d_dlnD = nullptr;
+    int ntab = 0;
+    double amintab = 0.0, amaxtab = 0.0, D_ainfty = 0.0, D_a0 = 0.0;
+    double HD_Hainfty = 0.0, HD_Ha0 = 0.0, cosmo_Om = 0.0, cosmo_OL = 0.0;
+    void* d_cat_ws = nullptr;      // flags, indices and CUB temp of the catalog kernels
+    size_t cat_ws_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked,
                                             // [8] (int32) device status word

@@ -303,6 +303,70 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
 #define HT_TUNE_FFT_PATH 4
 HT_API int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value);
 
+/* ------------------------------------------------ lightcone and halo records ---- */
+
+/* Cosmology tables of a run, built once on the host and copied into the context:
+ * the chi -> z table of build_chi_to_z (src/Cosmology/Cosmology.jl:334-347; chi ascending,
+ * Mpc/h) and the linear-growth tables of Dlinear_tables (Cosmology.jl:159-283). */
+typedef struct {
+    const double* chi;        /* comoving distance [n_chi], ascending */
+    const double* zchi;       /* redshift of each entry [n_chi] */
+    int32_t n_chi;
+    double z_max;             /* chi_to_z's clamp (the table's z_max) */
+    const double* atab;       /* scale factors [ntab], ascending */
+    const double* D_atab;     /* D(a)/a [ntab] */
+    const double* dlnD_dlna;  /* [ntab] */
+    int32_t ntab;
+    double amintab, amaxtab, D_ainfty, D_a0, HD_Hainfty, HD_Ha0;
+    double Om, OL;            /* omega_m_a of the 2LPT coefficient (MultiResolution.jl:734) */
+} ht_cosmo;
+
+/* Copy the tables (host arrays) into the context; required before the two calls below. */
+HT_API int ht_ctx_set_cosmo(ht_ctx* ctx, const ht_cosmo* cosmo);
+
+/* Geometry of a tile: side n (cells, buffer included), centre (Mpc/h), cell size. */
+typedef struct {
+    int32_t n;
+    double xbx, ybx, zbx;
+    double alatt;
+} ht_tile_geom;
+
+/* Per-peak lightcone state before the shell collapse (MultiResolution.jl:1097-1130):
+ * position x = xbx + alatt (i - (n+1)/2) (ext/CUDAExt.jl:3039-3046, FP64), z = chi_to_z(
+ * |x - obs|) (Cosmology.jl:354-385), ZZon = Float32(1 + z), fcrit = Float32(fsc_of_z(z))
+ * (RadialShell.jl:181-195).  Peaks with z <= z_max are kept: their 0-based indices, in
+ * order, go to d_keep and their number to *d_nkeep (device Int64).  d_i/d_j/d_k are the
+ * peak scan's 1-based cells; d_z may be NULL. */
+HT_API int ht_peak_lightcone(ht_ctx* ctx, const int32_t* d_i, const int32_t* d_j,
+                             const int32_t* d_k, int64_t npeaks, const ht_tile_geom* geom,
+                             const double* obs, double z_max, double* d_z, float* d_ZZon,
+                             float* d_fcrit, int32_t* d_keep, int64_t* d_nkeep,
+                             void* stream);
+
+/* The peaks of one collapse call, as packing reads them (device arrays). */
+typedef struct {
+    const int32_t* i;
+    const int32_t* j;
+    const int32_t* k;
+    const double* Rf;         /* filter radius (Mpc/h) */
+    const float* FcRf;        /* delta_s at the peak (PeakCandidate.delta) */
+    const float* d2Rf;        /* lapd_s at the peak; NULL: zeros */
+    const double* z;          /* per-peak redshift (lightcone); NULL: one ZZon for all */
+    int64_t npeaks;
+} ht_catalog_peaks;
+
+/* Halo records of the collapsed peaks (RTHL > 0, and z <= z_max on a lightcone), in peak
+ * order (MultiResolution.jl:1159-1219): HaloRecord rows of 11 Float32 when ioutshear == 0,
+ * ExtHaloRecord rows of 33 otherwise (src/IO/Catalog.jl:4-48): position, Sbar D(a),
+ * RTHL alatt, Sbar2 (-3/7) Om(a)^(-1/143) D(a)^2 (ilpt >= 2, else 0), Fbarx, and for the
+ * extended rows e_v, p_v, strain (11,22,33,23,13,12), d2F, zvir_half, gradpk, gradpkf, Rf,
+ * FcRf, d2Rf, gradpkrf.  D(a) = Dlinear_ab(1 / (1 + z)) (Cosmology.jl:286-306).  At most
+ * `cap` rows are written; *d_nhalo (device Int64) receives the number of halos. */
+HT_API int ht_pack_halos(ht_ctx* ctx, const ht_catalog_peaks* peaks, const ht_results* res,
+                         const ht_tile_geom* geom, double ZZon, double z_max, int32_t ilpt,
+                         int32_t ioutshear, float* d_records, int64_t cap, int64_t* d_nhalo,
+                         void* stream);
+
 /* ------------------------------------------------------ learned walk bracket ---- */
 
 /* A 12 -> 64 -> 64 -> 64 -> 2 MLP predicting the 10 % and 90 % quantiles of the radius at
