@@ -8,8 +8,9 @@ carried) and the radial-shell collapse, for one tile per GPU (weak scaling: N GP
 independent tiles, no collective on the data path).  A step is one tile's halo-finding
 stage as run_multitile_split performs it (MultiResolution.jl:1015-1219) with
 peak_find_tile_gpu's smoothing (ext/CUDAExt.jl:2951-3012): one rfft of the tile, then per
-filter the window + cuFFT C2R of the tile (ht_smooth_tile) and the peak scan, then the
-cell-record pack and the shell collapse of every peak in one launch.
+filter the window + inverse FFT of the tile (the pencil passes at 576/1152, else
+ht_smooth_tile) and the peak scan, then the cell-record pack, the shell collapse of every
+peak in one launch, and the HaloRecord rows of the collapsed peaks (ht_pack_halos).
 
 Inputs are seeded synthetic fields (BBKS LambdaCDM, Threefry noise, 2LPT), generated on
 the device before timing; they are far larger than the 126 MB L2, so no flush is needed.
@@ -190,6 +191,13 @@ class Workload:
         if mode == "learned":
             self.model = ht.bracket.BracketModel.load(device=device)
         self.pencil = ht.HaloFinder.pencil_supported(self.nt)
+        # the stage ends with the halo records of the collapsed peaks (MultiResolution.jl:
+        # 1159-1219): cosmology tables once, records packed on the device every step
+        cat = ht.catalog
+        cp = cat.CosmologyParams(Om=0.31, OB=0.049, OL=0.69, h=0.68, ns=0.965, s8=0.81)
+        cat.set_cosmology(self.finder, cp, cat.build_chi_to_z(cp, z_max=3.0, npts=200),
+                          cat.dlinear_tables(cp))
+        self.halos = None
 
     def smooth(self, Rf):
         if getattr(self, "_ds", None) is None:
@@ -292,6 +300,15 @@ class Workload:
                             mask=self.mask, mode=self.mode, out=self.results, cost=cost)
         if ev is not None:
             ev["walk"][1].record()
+        pks = {"i": pi, "j": pj, "k": pk, "Rf": Rf, "FcRf": self.peaks["delta"][:npk],
+               "d2Rf": None, "z": None}
+        if ev is not None and "records" in ev:
+            ev["records"][0].record()
+        self.halos = self.ht.catalog.pack_halos(self.finder, pks, self.results, self.nt,
+                                                (0.0, 0.0, 0.0), self.alatt, ZZon=self.ZZon,
+                                                ilpt=2, ioutshear=0)
+        if ev is not None and "records" in ev:
+            ev["records"][1].record()
         return npk
 
     def time_walk(self, reps=2):
@@ -359,7 +376,7 @@ def run_ours(args, rank, world, device):
     nf = len(W.filters)
     mk = lambda: torch.cuda.Event(enable_timing=True)
     evs = [{"pf": [(mk(), mk()) for _ in range(nf)], "pack": (mk(), mk()),
-            "walk": (mk(), mk())} for _ in range(args.steps)]
+            "walk": (mk(), mk()), "records": (mk(), mk())} for _ in range(args.steps)]
     start, end = mk(), mk()
     start.record()
     tot_peaks = 0
@@ -376,6 +393,7 @@ def run_ours(args, rank, world, device):
     pf_ms = sum(a.elapsed_time(b) for e in evs for a, b in e["pf"][:npf]) / args.steps
     pack_ms = sum(e["pack"][0].elapsed_time(e["pack"][1]) for e in evs) / args.steps
     walk_ms = sum(e["walk"][0].elapsed_time(e["walk"][1]) for e in evs) / args.steps
+    rec_ms = sum(e["records"][0].elapsed_time(e["records"][1]) for e in evs) / args.steps
     if dist:
         t = torch.tensor([t_ms, float(tot_peaks)], dtype=torch.float64, device=device)
         tmax = t.clone()
@@ -404,13 +422,15 @@ def run_ours(args, rank, world, device):
         "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
         "config": {"workload": args.workload, "desc": W.wl["desc"], "mode": args.mode,
                    "cuda_graph": bool(args.graph), "autotuned": W.tuned,
-                   "peaks_per_step": W.npeaks, "nhunt": W.nhunt, "nshells": W.finder.nshells,
+                   "peaks_per_step": W.npeaks, "halos_per_step": int(W.halos.shape[0]),
+                   "nhunt": W.nhunt, "nshells": W.finder.nshells,
                    "fcrit": W.fcrit, "l2": "inputs (43 GB of fields) >> 126 MB L2, no flush",
                    "parallelism": f"tile-per-GPU x{world}"},
         "breakdown_ms": {"peakfind_kernels" if W.graph is None else
                          "smoothing_and_peakfind_graph": pf_ms, "pack": pack_ms,
-                         "shell_walk": walk_ms,
-                         "smoothing_fft_and_rest": ms_per_step - pf_ms - pack_ms - walk_ms},
+                         "shell_walk": walk_ms, "halo_records": rec_ms,
+                         "smoothing_fft_and_rest": ms_per_step - pf_ms - pack_ms - walk_ms -
+                         rec_ms},
         "hot_path_peaks_per_s": W.npeaks / ((pf_ms + pack_ms + walk_ms) / 1e3),
         "roofline": {"kernel": "walk_kernel", "bound": "hbm", "achieved": achieved,
                      "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
@@ -418,9 +438,9 @@ def run_ours(args, rank, world, device):
                      "alg_bytes_per_launch": alg_bytes, "cells_walked": cells},
         # ours per step: per filter the window table + 3 transform kernels (pencil passes,
         # or the transposed path's window/transpose kernels) and 4 peak-scan kernels; per
-        # step the pencil transpose, pack, order keys, walk (+ features and MLP in learned
-        # mode); cuFFT and CUB launches not counted
-        "gpu_launches": int(args.steps * (8 * nf + (1 if W.pencil else 0) + 3 +
+        # step the pencil transpose, pack, order keys, walk, halo flags and records (+
+        # features and MLP in learned mode); cuFFT and CUB launches not counted
+        "gpu_launches": int(args.steps * (8 * nf + (1 if W.pencil else 0) + 5 +
                                           (2 if args.mode == "learned" else 0))),
         "clocks": ck,
         "e2e": e2e,
@@ -432,7 +452,7 @@ def run_ours(args, rank, world, device):
 def run_e2e(ht, W, args):
     """Same step through the public host-buffer API: fields start in pinned host memory and
     are copied into the device tile inside the timed region, and all results (peaks, the 14
-    result arrays and the mask) are read back into pinned host buffers.  delta is copied
+    result arrays, the mask and the halo records) are read back into pinned host buffers.  delta is copied
     first; the six displacement fields, first needed by the pack, copy on a second stream
     while the peak finding runs."""
     import torch
@@ -447,6 +467,7 @@ def run_e2e(ht, W, args):
     out_host = {n: torch.empty(out_count(g, n, W.npeaks), dtype=getattr(W, g)[n].dtype)
                 .pin_memory() for g, n in names}
     out_host["mask"] = torch.empty(W.mask.shape, dtype=W.mask.dtype).pin_memory()
+    out_host["halos"] = torch.empty(W.halos.numel(), dtype=torch.float32).pin_memory()
     side = torch.cuda.Stream()
     main = torch.cuda.current_stream()
     d2h = 0
@@ -482,6 +503,11 @@ def run_e2e(ht, W, args):
             d2h += cnt * src.element_size()
         out_host["mask"].copy_(W.mask, non_blocking=True)
         d2h += W.mask.numel() * W.mask.element_size()
+        nh = W.halos.numel()
+        if out_host["halos"].numel() < nh:
+            out_host["halos"] = torch.empty(nh, dtype=torch.float32).pin_memory()
+        out_host["halos"][:nh].copy_(W.halos.reshape(-1), non_blocking=True)
+        d2h += nh * 4
         e[3].record()
         torch.cuda.synchronize()
         parts["h2d_delta"] += e[0].elapsed_time(e[1])
