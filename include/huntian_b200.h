@@ -28,6 +28,13 @@
  *   ht_smooth_tile      -> one filter of ext/CUDAExt.jl:2985-2989 (copy + window +
  *                          irfft of the tile's own rfft, as peak_find_tile_gpu does)
  *   ht_smooth_filter    -> the same for a periodic box delivered as a wrapped tile
+ *   ht_spectrum_pencil +
+ *   ht_smooth_pencil    -> the loop over filters of ext/CUDAExt.jl:2951-2989 with the
+ *                          tile's spectrum kept (transposed once) across filters
+ *   ht_peak_lightcone   -> the per-peak host loop of src/MultiResolution.jl:1097-1130
+ *                          (peak_redshift, fsc_of_z, the z_max cut)
+ *   ht_pack_halos       -> the record loop of src/MultiResolution.jl:1159-1219
+ *                          (HaloRecord / ExtHaloRecord, src/IO/Catalog.jl:4-48)
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  */
