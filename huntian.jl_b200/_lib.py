@@ -42,7 +42,7 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
            "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
            "ht_bracket_adam", "ht_ctx_tune", "ht_ctx_set_cosmo", "ht_peak_lightcone",
-           "ht_pack_halos")
+           "ht_pack_halos", "ht_merge_halos", "ht_finalize_eulerian")
 
 
 class HTError(RuntimeError):
@@ -183,6 +183,10 @@ def load() -> C.CDLL:
     L.ht_pack_halos.restype = C.c_int
     L.ht_pack_halos.argtypes = [_P, C.POINTER(HtCatalogPeaks), C.POINTER(HtResults),
                                 C.POINTER(HtTileGeom), dbl, dbl, i32, i32, _P, i64, _P, _P]
+    L.ht_merge_halos.restype = C.c_int
+    L.ht_merge_halos.argtypes = [_P, _P, i64, i32, i32, i32, _P, _P, _P]
+    L.ht_finalize_eulerian.restype = C.c_int
+    L.ht_finalize_eulerian.argtypes = [_P, _P, i64, i32, _P, i32, dbl, _P]
     _lib = L
     return L
 

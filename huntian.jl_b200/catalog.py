@@ -8,7 +8,10 @@ Mirrors the host loops that follow the two GPU entry points in the reference til
 * the HaloRecord / ExtHaloRecord rows of the collapsed peaks (MultiResolution.jl:1159-1219,
   src/IO/Catalog.jl:4-48), with the linear growth factor D(a) of each peak's redshift
   (`pack_halos`);
-* the .pksc catalog format (Catalog.jl:48-110: `write_pksc`, `read_pksc`).
+* the .pksc catalog format (Catalog.jl:48-110: `write_pksc`, `read_pksc`);
+* the merge step that follows on the catalog: Lagrangian exclusion and volume reduction
+  (Merger.merge_catalog) and the Eulerian finalisation (Merger.finalize_eulerian)
+  (`merge_halos`, `finalize_eulerian`).
 
 The cosmology tables (chi -> z, Dlinear) are built once per run on the host, as the
 reference does (Cosmology.jl:159-283, 341-347), and copied into the library context
@@ -230,6 +233,37 @@ def pack_halos(finder, peaks: dict, results: dict, n: int, centre, alatt: float,
                                     float(ZZon), float(z_max), int(ilpt), int(ioutshear),
                                     out.data_ptr(), rows, nh.data_ptr(), _stream(stream)))
     return out[:min(int(nh.item()), rows)]
+
+
+def merge_halos(finder, records: torch.Tensor, *, volume_reduction: bool = False,
+                fortran_ties: bool = False, stream=None) -> torch.Tensor:
+    """ht_merge_halos (Merger.merge_catalog, Merger.jl:38-104): Lagrangian exclusion (and
+    optionally volume reduction) of (nhalo, 11 | 33) Float32 device records; returns the
+    survivors in input order with their RTHL (reduced when volume_reduction)."""
+    rec = records.contiguous()
+    n, width = (int(rec.shape[0]), int(rec.shape[1])) if rec.dim() == 2 else (0, 11)
+    out = torch.empty((max(n, 1), width), dtype=torch.float32, device=rec.device)
+    nout = torch.zeros(1, dtype=torch.int64, device=rec.device)
+    check(_lib.load().ht_merge_halos(finder.handle, rec.data_ptr() if n else None, n, width,
+                                     int(bool(volume_reduction)), int(bool(fortran_ties)),
+                                     out.data_ptr(), nout.data_ptr(), _stream(stream)))
+    return out[:int(nout.item())]
+
+
+def finalize_eulerian(finder, records: torch.Tensor, obs=(0.0, 0.0, 0.0), *, ievol: int = 1,
+                      z_out: float = 0.0, stream=None) -> torch.Tensor:
+    """ht_finalize_eulerian (Merger.finalize_eulerian, Merger.jl:114-146), in place on a
+    merged raw catalog: Eulerian positions and km/s velocities.  Uses the chi -> z and
+    growth tables of set_cosmology (the reference builds its chi table with z_max = 10)."""
+    n = int(records.shape[0]) if records.dim() == 2 else 0
+    if n == 0:
+        return records
+    assert records.is_contiguous() and records.dtype == torch.float32
+    o = (C.c_double * 3)(*[float(v) for v in obs])
+    check(_lib.load().ht_finalize_eulerian(finder.handle, records.data_ptr(), n,
+                                           int(records.shape[1]), C.cast(o, C.c_void_p),
+                                           int(ievol), float(z_out), _stream(stream)))
+    return records
 
 
 # --------------------------------------------------------------- .pksc files ----

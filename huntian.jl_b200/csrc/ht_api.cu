@@ -223,7 +223,7 @@ static void free_ctx(ht_ctx* c) {
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
                     c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_ftw, c->d_queue,
                     c->d_stats, c->d_chi, c->d_zchi, c->d_atab, c->d_Da, c->d_dlnD,
-                    c->d_cat_ws};
+                    c->d_cat_ws, c->d_merge_ws, c->d_merge_cells, c->d_merge_scan};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete c;

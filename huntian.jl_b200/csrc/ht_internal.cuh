@@ -103,6 +103,12 @@ struct ht_ctx {
     double HD_Hainfty = 0.0, HD_Ha0 = 0.0, cosmo_Om = 0.0, cosmo_OL = 0.0;
     void* d_cat_ws = nullptr;      // flags, indices and CUB temp of the catalog kernels
     size_t cat_ws_bytes = 0;
+    void* d_merge_ws = nullptr;    // halo merging: per-halo arrays and CUB temp
+    size_t merge_ws_bytes = 0;
+    void* d_merge_cells = nullptr; // halo merging: cell counts and starts
+    size_t merge_cells_bytes = 0;
+    void* d_merge_scan = nullptr;  // halo merging: scan temp of large cell tables
+    size_t merge_scan_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked,
                                             // [8] (int32) device status word

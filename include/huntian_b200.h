@@ -35,6 +35,9 @@
  *                          (peak_redshift, fsc_of_z, the z_max cut)
  *   ht_pack_halos       -> the record loop of src/MultiResolution.jl:1159-1219
  *                          (HaloRecord / ExtHaloRecord, src/IO/Catalog.jl:4-48)
+ *   ht_merge_halos      -> src/Merger/Merger.jl:38-104 `merge_catalog` (exclusion and
+ *                          volume reduction, src/Merger/Exclusion.jl)
+ *   ht_finalize_eulerian -> src/Merger/Merger.jl:114-146 `finalize_eulerian`
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  */
@@ -373,6 +376,28 @@ HT_API int ht_pack_halos(ht_ctx* ctx, const ht_catalog_peaks* peaks, const ht_re
                          const ht_tile_geom* geom, double ZZon, double z_max, int32_t ilpt,
                          int32_t ioutshear, float* d_records, int64_t cap, int64_t* d_nhalo,
                          void* stream);
+
+/* Lagrangian exclusion of a halo catalog (src/Merger/Merger.jl:38-104 merge_catalog,
+ * src/Merger/Exclusion.jl:99-140): halos in decreasing radius (ties by x, y, z, then input
+ * order); a surviving halo removes every later halo whose centre lies inside its radius.
+ * With volume_reduction, overlapping survivors then shrink by their cap volumes
+ * (Exclusion.jl:152-206; fortran_ties counts an equal-radius pair twice), and halos left
+ * with no volume are removed.  d_records: nhalo rows of `width` (11 or 33) Float32 in the
+ * Catalog layout (x, y, z at 0-2, RTHL at 6).  d_out receives the survivors in input order
+ * with their (possibly reduced) RTHL, at most nhalo rows; *d_nout (device Int64) their
+ * number.  Deterministic except the last bits of reduced radii (the cap volumes are summed
+ * with atomics). */
+HT_API int ht_merge_halos(ht_ctx* ctx, const float* d_records, int64_t nhalo, int32_t width,
+                          int32_t volume_reduction, int32_t fortran_ties, float* d_out,
+                          int64_t* d_nout, void* stream);
+
+/* Eulerian positions and peculiar velocities of a merged raw catalog, in place
+ * (Merger.jl:114-146 finalize_eulerian): x = q + d1 + d2, v = a 100 E(a) f(a) (d1 + 2 d2)
+ * km/s with f = dlnD/dlna from the context's growth tables, the 2LPT fields zeroed; a from
+ * the chi -> z table at the Eulerian distance to obs (ievol = 1) or 1 / (1 + z_out).
+ * Requires ht_ctx_set_cosmo. */
+HT_API int ht_finalize_eulerian(ht_ctx* ctx, float* d_records, int64_t nhalo, int32_t width,
+                                const double* obs, int32_t ievol, double z_out, void* stream);
 
 /* ------------------------------------------------------ learned walk bracket ---- */
 

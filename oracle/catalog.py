@@ -11,7 +11,11 @@ with Float32 roundings where the reference converts, of:
 * omega_m_a (Cosmology.jl:52),
 * the lightcone loop before the collapse (src/MultiResolution.jl:1097-1130) and the record
   loop after it (MultiResolution.jl:1159-1219) with the field order of HaloRecord /
-  ExtHaloRecord (src/IO/Catalog.jl:4-48).
+  ExtHaloRecord (src/IO/Catalog.jl:4-48),
+* merge_catalog with lagrangian_exclusion! and volume_reduction! (src/Merger/Merger.jl:38-104,
+  src/Merger/Exclusion.jl:81-206) and finalize_eulerian (Merger.jl:114-146); the
+  neighbour search is a k-d tree instead of the linked-list hash (both are exhaustive
+  within the radius, so the survivors do not depend on it).
 
 fsc_of_z is the C oracle's (RadialShell.jl:181-195).  The cosmology tables themselves are
 inputs (built by the host code the reference runs once per run).
@@ -171,3 +175,116 @@ def halo_records(peaks: dict, res: dict, n: int, centre, alatt: float, growth, O
         rows.append(np.array(rec, np.float32))
     width = 33 if ioutshear >= 1 else 11
     return np.array(rows, np.float32).reshape(-1, width)
+
+
+def growth_f(g, ai: float) -> float:
+    """Second value of Dlinear_ab: dlnD/dlna with the same Lagrange weights."""
+    atab, ftab, ntab = g.atab, g.dlnD_dlnatab, len(g.atab)
+    if g.amintab < ai < g.amaxtab:
+        kk = hunt(atab, ai)
+        if kk < 2 or kk >= ntab:
+            nlint, kkl = 2, max(kk - 1, 1)
+        else:
+            nlint, kkl = 4, max(kk - 2, 1)
+        xa = [float(atab[kkl - 1 + q]) for q in range(nlint)]
+        va = [float(ftab[kkl - 1 + q]) for q in range(nlint)]
+        x = ai
+        if nlint == 4:
+            def coef(i, a_, b_, c_):
+                return (x - xa[a_]) / (xa[i] - xa[a_]) * (x - xa[b_]) / (xa[i] - xa[b_]) * \
+                    (x - xa[c_]) / (xa[i] - xa[c_])
+            a1, a2, a3, a4 = coef(0, 1, 2, 3), coef(1, 0, 2, 3), coef(2, 0, 1, 3), coef(3, 0, 1, 2)
+            return a1 * va[0] + a2 * va[1] + a3 * va[2] + a4 * va[3]
+        a1 = (x - xa[1]) / (xa[0] - xa[1])
+        return a1 * va[0] + (1.0 - a1) * va[1]
+    return g.HD_Ha0 if ai >= g.amaxtab else g.HD_Hainfty
+
+
+def sphere_overlap(d: float, r1: float, r2: float):
+    """Exclusion.jl:81-97."""
+    if d >= r1 + r2 or d <= abs(r1 - r2):
+        return 0.0, 0.0
+    h1 = (r2 - r1 + d) * (r2 + r1 - d) / (2.0 * d)
+    h2 = (r1 - r2 + d) * (r1 + r2 - d) / (2.0 * d)
+    return (math.pi / 3.0) * (h1 * h1) * (3.0 * r1 - h1), (math.pi / 3.0) * (h2 * h2) * (3.0 * r2 - h2)
+
+
+def merge_catalog(rec, volume_reduction: bool = False, fortran_ties: bool = False):
+    """Merger.jl:38-104: survivors (input order) with their RTHL, as Float32 rows."""
+    from scipy.spatial import cKDTree
+    rec = np.asarray(rec, np.float32)
+    n = rec.shape[0]
+    if n == 0:
+        return rec.copy()
+    x, y, z = (rec[:, c].astype(np.float64) for c in range(3))
+    r = rec[:, 6].astype(np.float64)
+    xl, yl, zl, rl = x.tolist(), y.tolist(), z.tolist(), r.tolist()
+    order = sorted(range(n), key=lambda i: (-rl[i], xl[i], yl[i], zl[i]))
+    tree = cKDTree(np.stack([x, y, z], 1))
+    surv = [True] * n
+
+    def dist(i, j):
+        dx, dy, dz = xl[j] - xl[i], yl[j] - yl[i], zl[j] - zl[i]
+        return math.sqrt(dx * dx + dy * dy + dz * dz)
+
+    for i in order:                              # lagrangian_exclusion! (Exclusion.jl:99-140)
+        if not surv[i]:
+            continue
+        ri = rl[i]
+        for j in tree.query_ball_point((xl[i], yl[i], zl[i]), ri * (1 + 1e-9) + 1e-9):
+            if j != i and surv[j] and ri >= rl[j] and dist(i, j) < ri:
+                surv[j] = False
+    new_r = list(rl)
+    if volume_reduction:                         # volume_reduction! (Exclusion.jl:152-206)
+        rank = [0] * n
+        for k, i in enumerate(order):
+            rank[i] = k
+        dV = [0.0] * n
+        for i in order:
+            if not surv[i]:
+                continue
+            ri = rl[i]
+            for j in tree.query_ball_point((xl[i], yl[i], zl[i]), 2 * ri * (1 + 1e-9) + 1e-9):
+                if j != i and surv[j] and rank[j] > rank[i]:
+                    rj = rl[j]
+                    d = dist(i, j)
+                    if d < ri + rj:
+                        v1, v2 = sphere_overlap(d, ri, rj)
+                        w = 2.0 if (fortran_ties and rj == ri) else 1.0
+                        dV[i] += w * v1
+                        dV[j] += w * v2
+        for i in range(n):
+            if not surv[i]:
+                continue
+            vol = 4 * math.pi / 3 * (rl[i] * rl[i] * rl[i]) - dV[i]
+            if vol <= 0.0:
+                surv[i], new_r[i] = False, 0.0
+            else:
+                new_r[i] = math.cbrt(vol * 3 / (4 * math.pi))
+    keep = [i for i in range(n) if surv[i]]
+    out = rec[keep].copy()
+    out[:, 6] = np.array([new_r[i] for i in keep], np.float32)
+    return out
+
+
+def finalize_eulerian(rec, growth, Om: float, OL: float, obs, chis, zs, zmax_tab: float,
+                      ievol: int = 1, z_out: float = 0.0):
+    """Merger.jl:114-146 on Float32 rows (a copy is returned)."""
+    out = np.array(rec, np.float32, copy=True)
+    a_snap = 1.0 / (1.0 + z_out)
+    for h in range(out.shape[0]):
+        q = out[h]
+        d1 = [float(q[3]), float(q[4]), float(q[5])]
+        d2 = [float(q[7]), float(q[8]), float(q[9])]
+        e = [float(q[c]) + d1[c] + d2[c] for c in range(3)]
+        a = a_snap
+        if ievol == 1:
+            dx, dy, dz = e[0] - obs[0], e[1] - obs[1], e[2] - obs[2]
+            rr = math.sqrt(dx * dx + dy * dy + dz * dz)
+            a = 1.0 / (1.0 + chi_to_z(chis, zs, zmax_tab, rr)) if rr > 0 else 1.0
+        E = math.sqrt(Om * a ** -3 + OL)
+        vfac = a * 100.0 * E * growth_f(growth, a)
+        q[0:3] = np.array(e, np.float32)
+        q[3:6] = np.array([vfac * (d1[c] + 2 * d2[c]) for c in range(3)], np.float32)
+        q[7:10] = 0.0
+    return out
