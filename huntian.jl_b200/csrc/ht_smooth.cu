@@ -550,8 +550,8 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
 //   X  half-length real packing, FFT of n/2:     C (z, y, kx)   -> out (z, y, x)
 // B holds only z in [zlo, zlo + Rz) and C only those z with y in [ylo, ylo + Ry): just the
 // output rows (z, y) in that range are written.  A peak scan of the region
-// [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.  C rows carry one pad
-// element (n/2 + 2 complex values) so that every row starts on 16 bytes.
+// [lo + 1, hi - 1)^3 reads the rows (z, y) in [lo, hi)^2 only.  C rows are padded to a
+// multiple of 16 complex values (128 bytes).
 //
 // All three kernels are persistent; columns and rows arrive by 1-D bulk copies
 // (cp.async.bulk, completing on an mbarrier that one thread polls with a bounded wait).
@@ -580,11 +580,20 @@ constexpr size_t pencil_smem_yz() {
     return (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
 }
 
-// X: a warp's slot holds 33 TH complex values rounded up to even (16-byte slots; a padded
-// C row of M + 2 values fits), two slots per warp
+// C rows hold the n/2 + 1 modes of one (z, y) padded to a multiple of 16 complex values
+// (128 bytes): the Y pass stores 64-byte pieces into them, which then start on 64-byte
+// boundaries and cover whole 32-byte sectors (an unaligned pitch made every piece touch a
+// third, partly written sector).
+__host__ __device__ constexpr int pencil_row_pitch(int n) {
+    return (n / 2 + 1 + 15) & ~15;
+}
+
+// X: a warp's slot holds 33 TH complex values rounded up to even (16-byte slots), or a
+// padded C row if that is longer, two slots per warp
 template <int TH>
 __host__ __device__ constexpr int pencil_slot_x() {
-    return (33 * TH + 1) & ~1;
+    return ((33 * TH + 1) & ~1) > pencil_row_pitch(64 * TH) ? ((33 * TH + 1) & ~1)
+                                                             : pencil_row_pitch(64 * TH);
 }
 template <int TH>
 constexpr size_t pencil_smem_x() {
@@ -784,7 +793,8 @@ __global__ void __launch_bounds__(256, 2) py_kernel(
 
 // TH = n / 64: the packed rows have M = n / 2 = 32 TH points.  Every warp streams rows
 // r = global warp, + total warps, ... through two slots: row r + stride is copied into the
-// other slot while row r is packed, transformed and stored.
+// other slot while row r is packed, transformed and stored.  C rows start NKP values apart;
+// a copy takes the first n/2 + 1 values rounded up to even (16 bytes).
 template <int TH>
 __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
                                                  float2* __restrict__ out, int NKP, int zlo,
@@ -794,14 +804,14 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
                                                  const float2* __restrict__ tw32,
                                                  int32_t* __restrict__ status) {
     constexpr int M = 32 * TH, N = 2 * M, S = pencil_slot_x<TH>();
-    static_assert(S >= M + 2, "a padded C row must fit a slot");
+    static_assert(S >= pencil_row_pitch(N) && S >= 33 * TH, "a padded C row must fit a slot");
     extern __shared__ __align__(128) float2 sm[];
     __shared__ __align__(8) unsigned long long bars[8][2];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     float2* slots = sm + w * 2 * S;
     unsigned long long* bar = bars[w];
     const long long stride = (long long)gridDim.x * 8;
-    const unsigned row_bytes = (unsigned)NKP * (unsigned)sizeof(float2);
+    const unsigned row_bytes = (unsigned)((M + 2) & ~1) * (unsigned)sizeof(float2);
     long long r = (long long)blockIdx.x * 8 + w;
     if (lane == 0) {
         htasync::bar_init(&bar[0], 1);
@@ -885,7 +895,7 @@ template <int T>
 static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, float2* d_out,
                          int zlo, int zhi, int ylo, int yhi, cudaStream_t st) {
     constexpr int n = 32 * T, TH = T / 2;
-    const int nk = n / 2 + 1, nkp = nk + 1, Rz = zhi - zlo, Ry = yhi - ylo;
+    const int nk = n / 2 + 1, nkp = pencil_row_pitch(n), Rz = zhi - zlo, Ry = yhi - ylo;
     const size_t smyz = pencil_smem_yz<T>(), smx = pencil_smem_x<TH>();
     HT_CUDA_TRY(cudaFuncSetAttribute(pz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "pz smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "py smem");
@@ -946,14 +956,15 @@ static int smooth_pencil_run(ht_ctx* ctx, const float2* P, float* d_out, int n, 
                              double Rf, int wsmooth, int zlo, int zhi, int ylo, int yhi,
                              cudaStream_t st) {
     const size_t nk = (size_t)n / 2 + 1;
-    const size_t cbytes = (nk + 1) * (size_t)(zhi - zlo) * (yhi - ylo) * sizeof(float2);
+    const size_t cbytes = (size_t)pencil_row_pitch(n) * (size_t)(zhi - zlo) * (yhi - ylo) *
+                          sizeof(float2);
     // C takes the first buffer; when P lives there too it must already be large enough
     // (a reallocation here would free P before the first pass reads it)
     if ((const void*)P == ctx->d_cwork && ctx->cwork_bytes < cbytes)
         return ht_fail(HT_ERR_STATE, "smooth_pencil_run: pencil buffer smaller than C");
     int rc = ht_grow(&ctx->d_cwork2, &ctx->cwork2_bytes,
                      nk * (size_t)(zhi - zlo) * n * sizeof(float2), "smoothing buffer 2");
-    if (rc == HT_OK)   // C rows carry one pad element
+    if (rc == HT_OK)   // C rows are padded to 128 bytes
         rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
     if (rc == HT_OK) rc = fused_tables(ctx, n);
     if (rc == HT_OK) rc = scaled_window_table(ctx, n, boxsize, Rf, wsmooth, st);
@@ -975,9 +986,9 @@ static int smooth_tile_pencil(ht_ctx* ctx, const void* d_delta_k, float* d_out, 
                               double boxsize, double Rf, int wsmooth, int zlo, int zhi,
                               cudaStream_t st) {
     const size_t nk = (size_t)n / 2 + 1;
-    // the buffer holds P, then C (rows of nk + 1 for z in [zlo, zhi), all y): size it for
+    // the buffer holds P, then C (padded rows for z in [zlo, zhi), all y): size it for
     // both before P is written
-    const size_t need = std::max(nk * n * n, (nk + 1) * (size_t)(zhi - zlo) * n) *
+    const size_t need = std::max(nk * n * n, (size_t)pencil_row_pitch(n) * (zhi - zlo) * n) *
                         sizeof(float2);
     int rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, need, "smoothing buffer");
     if (rc != HT_OK) return rc;

@@ -35,7 +35,7 @@ int main(int argc, char** argv) {
     // the bench's region: rows (z, y) in [63, 1089); the Y pass writes 64 y rows, the X pass
     // transforms 64 z planes of R rows
     const int lo = 63, R = n - 2 * lo, ry = 64, zx = 64;
-    const int nkp = n / 2 + 2;                        // padded C row
+    const int nkp = pencil_row_pitch(n);              // padded C row
     const long long rows = (long long)zx * R;
     const size_t pb = (size_t)n * nks * n * sizeof(float2);
     const size_t bb = (size_t)nks * R * n * sizeof(float2);
