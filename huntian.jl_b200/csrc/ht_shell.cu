@@ -195,19 +195,23 @@ struct Strain {
 // row of mp = 1 lists shells 2..U(1) with the atab4 weight 0.5 * W / rad[m1].  The
 // weighted sums are scaled by wRnor / rad[mp] (mp > 1) or aRnor (mp = 1) at the end, in
 // the reference's order.
-__device__ __noinline__ Strain kernel_strain(const WalkArgs& a, const double* __restrict__ P,
+__device__ __noinline__ Strain kernel_strain(const int32_t* __restrict__ wrow,
+                                             const int32_t* __restrict__ wm1,
+                                             const double* __restrict__ wwt,
+                                             const double* __restrict__ rad, double wRnor,
+                                             double aRnor, const double* __restrict__ P,
                                              int mp, int lo, int hi) {
     Strain s;
 #pragma unroll
     for (int i = 0; i < 6; ++i) s.E[i] = 0.0;
 #pragma unroll
     for (int i = 0; i < 3; ++i) { s.g[i] = 0.0; s.gf[i] = 0.0; }
-    const int e0 = __ldg(a.wrow + mp), e1 = __ldg(a.wrow + mp + 1);
+    const int e0 = __ldg(wrow + mp), e1 = __ldg(wrow + mp + 1);
     for (int e = e0; e < e1; ++e) {
-        const int m1 = __ldg(a.wm1 + e);
+        const int m1 = __ldg(wm1 + e);
         if (m1 > hi) break;
         if (m1 < lo) continue;
-        const double wt = __ldg(a.wwt + e);
+        const double wt = __ldg(wwt + e);
         const double hw = 0.5 * wt;
         const double* q = P + (size_t)m1 * kRec;
 #pragma unroll
@@ -218,7 +222,7 @@ __device__ __noinline__ Strain kernel_strain(const WalkArgs& a, const double* __
 #pragma unroll
         for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
     }
-    const double scale = mp > 1 ? a.wRnor / a.rad[mp] : a.aRnor;
+    const double scale = mp > 1 ? wRnor / rad[mp] : aRnor;
 #pragma unroll
     for (int i = 0; i < 6; ++i) s.E[i] *= scale;
 #pragma unroll
@@ -229,7 +233,9 @@ __device__ __noinline__ Strain kernel_strain(const WalkArgs& a, const double* __
 // kernel_strain's central branch over shells lo..hi computed directly (used for the
 // gradient at the filter scale when mrf = 1, whose window starts at the centre shell:
 // its weight 0.5 * W(0) / 0 is infinite and the reference's gradient is NaN).
-__device__ __noinline__ Strain kernel_strain_central(const WalkArgs& a,
+__device__ __noinline__ Strain kernel_strain_central(const double* __restrict__ rad,
+                                                     const double* __restrict__ akk,
+                                                     double aRnor,
                                                      const double* __restrict__ P, int lo,
                                                      int hi) {
     Strain s;
@@ -238,13 +244,13 @@ __device__ __noinline__ Strain kernel_strain_central(const WalkArgs& a,
 #pragma unroll
     for (int i = 0; i < 3; ++i) { s.g[i] = 0.0; s.gf[i] = 0.0; }
     for (int m1 = lo; m1 <= hi; ++m1) {
-        const double r1 = a.rad[m1];
+        const double r1 = rad[m1];
         const double con = 100.0 * r1 * r1;
         const double fl = floor(con);
         const int icon = (int)fl;
         const double diff = con - fl;
         double aww = 0.0;
-        if (icon >= 0 && icon < 1100) aww = a.akk[icon] + diff * (a.akk[icon + 1] - a.akk[icon]);
+        if (icon >= 0 && icon < 1100) aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
         const double wt = 0.5 * aww / r1;
         const double hw = 0.5 * wt;
         const double* q = P + (size_t)m1 * kRec;
@@ -257,10 +263,23 @@ __device__ __noinline__ Strain kernel_strain_central(const WalkArgs& a,
         for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
     }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) s.E[i] *= a.aRnor;
+    for (int i = 0; i < 6; ++i) s.E[i] *= aRnor;
 #pragma unroll
-    for (int i = 0; i < 3; ++i) { s.g[i] *= a.aRnor; s.gf[i] *= a.aRnor; }
+    for (int i = 0; i < 3; ++i) { s.g[i] *= aRnor; s.gf[i] *= aRnor; }
     return s;
+}
+
+// The walk's arguments stay in the kernel's parameter space (constant bank): functions
+// that read them are inlined, and the out-of-line ones above receive the fields they use.
+// (A reference to the parameter block passed out of line makes every thread copy it to
+// local memory and read its fields from there.)
+__device__ __forceinline__ Strain strain_at(const WalkArgs& a, const double* P, int mp,
+                                            int lo, int hi) {
+    return kernel_strain(a.wrow, a.wm1, a.wwt, a.rad, a.wRnor, a.aRnor, P, mp, lo, hi);
+}
+__device__ __forceinline__ Strain strain_central(const WalkArgs& a, const double* P, int lo,
+                                                 int hi) {
+    return kernel_strain_central(a.rad, a.akk, a.aRnor, P, lo, hi);
 }
 
 // Ascending eigenvalues of a symmetric 3x3 matrix in FP64 by the trigonometric solution
@@ -293,7 +312,7 @@ __device__ __noinline__ void eig3(const double* E, double* lam) {
 
 // Trilinear collapse-table lookup, -1 (out_val) outside the closed box
 // (CollapseTable.jl:126-138), in FP64 over the Float32 table.
-__device__ __noinline__ double interp3(const WalkArgs& a, double x, double y, double z) {
+__device__ __forceinline__ double interp3(const WalkArgs& a, double x, double y, double z) {
     if (!(x >= a.X1 && x <= a.X2 && y >= a.Y1 && y <= a.Y2 && z >= a.Z1 && z <= a.Z2))
         return a.out_val;
     double tx = (x - a.X1) / ((a.X2 - a.X1) / (a.nx - 1));
@@ -343,7 +362,7 @@ struct Step {
 __device__ __forceinline__ Step eval_step(const WalkArgs& a, const double* P, int mp, int m,
                                           bool force_minus_one) {
     Step st;
-    st.k = kernel_strain(a, P, mp, 1, m);
+    st.k = strain_at(a, P, mp, 1, m);
     const Shape sh = shape_of(st.k.E);
     st.trace = sh.trace;
     st.zvir = -1.0;
@@ -357,7 +376,8 @@ __device__ __forceinline__ Step eval_step(const WalkArgs& a, const double* P, in
     return st;
 }
 
-__device__ void write_no_collapse(const WalkArgs& a, long long p, const Group& g) {
+__device__ __forceinline__ void write_no_collapse(const WalkArgs& a, long long p,
+                                                  const Group& g) {
     const ht_results& o = a.out;
     for (int i = g.t; i < 9; i += g.G) o.strain[9 * p + i] = 0.f;
     if (g.t < 3) {
@@ -447,7 +467,7 @@ __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck
 // mrf, the shell whose gradient is reported as gradpkrf (RadialShell.jl:449-464 for the
 // CPU convention, ShellAnalysisGPU.jl:234-254 for the GPU one): the first shell s >= 2
 // minimising |r2[s] - (Rf/alatt)^2| below 10, minus the lag of the reference counters.
-__device__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
+__device__ __forceinline__ int find_mrf(const WalkArgs& a, double R2, int smax, int conv) {
     int lo = 2, hi = smax, first_ge = smax + 1;
     while (lo <= hi) {
         int mid = (lo + hi) >> 1;
@@ -517,7 +537,7 @@ __device__ __forceinline__ int group_size(const WalkArgs& a, long long p) {
 }
 
 template <bool PACKED>
-__device__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P,
+__device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P,
                              double* __restrict__ R, const Group& g) {
     const double* rad = a.rad;
     const int G = g.G, t = g.t, RP = G + 1;
@@ -624,8 +644,8 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
     // starts at the centre shell
     double gradpkrf[3];
     {
-        const Strain k = bd.mrf > 1 ? kernel_strain(a, P, bd.mrf, 1, bd.need_rf)
-                                    : kernel_strain_central(a, P, 1, bd.need_rf);
+        const Strain k = bd.mrf > 1 ? strain_at(a, P, bd.mrf, 1, bd.need_rf)
+                                    : strain_central(a, P, 1, bd.need_rf);
         gradpkrf[0] = k.g[0]; gradpkrf[1] = k.g[1]; gradpkrf[2] = k.g[2];
     }
 
@@ -839,7 +859,11 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
         for (int jj0 = 0; jj0 < 10; jj0 += G) {
             const int jj = jj0 + t;   // 0-based radius index
             if (jj >= 10) continue;
-            const double rcur = RTHL * a.zh_frac[jj];
+            double zf = a.zh_frac[0];   // constant indices: the table stays in the parameters
+#pragma unroll
+            for (int q = 1; q < 10; ++q)
+                if (jj == q) zf = a.zh_frac[q];
+            const double rcur = RTHL * zf;
             const int mm1 = m - 1;
             int mupp_rc = 1;
             if (mm1 >= 2) {
@@ -856,8 +880,8 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
                 const int f = first_above(rad, 1, mm1, rcur);
                 m0_rc = f <= mm1 ? f : mm1;
             }
-            const Strain k = m0_rc > 1 ? kernel_strain(a, P, m0_rc, mlow_rc, mupp_rc)
-                                       : kernel_strain_central(a, P, mlow_rc, mupp_rc);
+            const Strain k = m0_rc > 1 ? strain_at(a, P, m0_rc, mlow_rc, mupp_rc)
+                                       : strain_central(a, P, mlow_rc, mupp_rc);
             const Shape sh = shape_of(k.E);
             const double Fc = P[(size_t)m0_rc * kRec + P_FBAR];
             const double poe = sh.e_v < 1e-5 ? 0.0 : sh.p_v / sh.e_v;
@@ -909,39 +933,57 @@ __device__ void process_peak(const WalkArgs& a, long long p, double* __restrict_
 // with its own G (lanes 8..31 idle for a G = 8 peak).  Group q of warp w owns scratch
 // slot 4 w + q.
 template <bool PACKED>
-__device__ void process_item(const WalkArgs& a, long long item, double* P0, double* W,
-                             int lane) {
+__device__ __forceinline__ void process_item(const WalkArgs& a, long long item, double* P0,
+                                             double* W, int lane) {
     const long long p0 = item * kPeaksPerItem;
     const int np = (int)min((long long)kPeaksPerItem, a.npeaks - p0);
     long long pid[kPeaksPerItem];
     int gs[kPeaksPerItem];
     bool all_small = np == kPeaksPerItem;
-    for (int k = 0; k < np; ++k) {
+#pragma unroll
+    for (int k = 0; k < kPeaksPerItem; ++k) {
         long long p = p0 + k;
-        if (a.order) {
+        if (k < np && a.order) {
             p = (long long)__ldg(a.order + p);
             if (p < 0 || p >= a.npeaks) p = -1;   // not a peak index: skipped
         }
-        pid[k] = p;
-        gs[k] = p >= 0 ? group_size(a, p) : 0;
+        pid[k] = k < np ? p : -1;
+        gs[k] = pid[k] >= 0 ? group_size(a, pid[k]) : 0;
         all_small = all_small && gs[k] == kSmallG;
     }
-    if (all_small) {
-        const int q = lane / kSmallG;
-        Group g{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
-        process_peak<PACKED>(a, pid[q], P0 + q * a.scratch_stride,
-                             W + q * group_smem_doubles(kSmallG), g);
-    } else {
-        for (int k = 0; k < np; ++k) {
-            if (gs[k] == 32) {
-                Group g{32, lane, 0, 0xffffffffu};
-                process_peak<PACKED>(a, pid[k], P0, W, g);
-            } else if (gs[k] == kSmallG && lane < kSmallG) {
-                Group g{kSmallG, lane, 0, (1u << kSmallG) - 1u};
-                process_peak<PACKED>(a, pid[k], P0, W, g);
-            }
-            __syncwarp();
+    // pid[i] / gs[i] for a run-time i, by selects (no local-memory array)
+    auto pick = [&](int i, long long& p, int& G) {
+        p = pid[0];
+        G = gs[0];
+#pragma unroll
+        for (int k = 1; k < kPeaksPerItem; ++k)
+            if (i == k) { p = pid[k]; G = gs[k]; }
+    };
+    // one call site of process_peak: four groups of 8 side by side, or the peaks one after
+    // the other with their own G
+    const int rounds = all_small ? 1 : np;
+    for (int k = 0; k < rounds; ++k) {
+        long long p;
+        int G;
+        Group g;
+        double* Pq = P0;
+        double* Wq = W;
+        bool run;
+        if (all_small) {
+            const int q = lane / kSmallG;
+            pick(q, p, G);
+            g = Group{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
+            Pq = P0 + q * a.scratch_stride;
+            Wq = W + q * group_smem_doubles(kSmallG);
+            run = true;
+        } else {
+            pick(k, p, G);
+            g = G == 32 ? Group{32, lane, 0, 0xffffffffu}
+                        : Group{kSmallG, lane, 0, (1u << kSmallG) - 1u};
+            run = G == 32 || (G == kSmallG && lane < kSmallG);
         }
+        if (run) process_peak<PACKED>(a, p, Pq, Wq, g);
+        __syncwarp();
     }
     __syncwarp();
 }

@@ -555,29 +555,44 @@ static int smooth_tile_fused(ht_ctx* ctx, const void* d_delta_k, float* d_out, i
 //
 // All three kernels are persistent; columns and rows arrive by 1-D bulk copies
 // (cp.async.bulk, completing on an mbarrier that one thread polls with a bounded wait).
-// Z and Y: a CTA takes 8 neighbouring columns (8 warps, one column each), reads them from
-// its shared-memory slot into registers, transforms, writes the 8 results back into the
-// same slot in lane-major order and stores them in 64-byte pieces of the next layout, then
-// requests the next item's columns; two CTAs per SM overlap one's copies with the other's
-// arithmetic (measured faster than one CTA per SM with a second slot).  X: every warp
-// streams rows through a two-slot ring of its own, the next row in flight while the
-// current one is transformed.
+// Z and Y: a CTA takes neighbouring columns (one warp each), reads them from its shared-
+// memory slot into registers, transforms, writes the results in lane-major order and
+// stores them in pieces of the next layout.  Z: 8 columns, the results reuse the slot, the
+// next item's columns are requested after the store, two CTAs per SM overlap one's copies
+// with the other's arithmetic (64-byte pieces; measured faster than 4 columns, and as fast
+// as one CTA per SM with a second slot).  Y: 4 columns with a separate result area, the
+// next columns requested as soon as the current ones sit in registers, three CTAs per SM
+// (measured 16 % faster than the Z shape on the full Y pass).  X: every warp streams rows
+// through a two-slot ring of its own, the next row in flight while the current one is
+// transformed.
 
 namespace {
 
-constexpr int kPencilCols = 8;   // columns (warps) per CTA in the Z and Y passes
+// Z / Y CTA shapes: COLS neighbouring columns (one warp each) per work item; SEP gives the
+// bulk-copy destination a buffer of its own, so that the next item's columns are requested
+// as soon as the current ones sit in registers (else the row-major outputs reuse the slot
+// and the request follows the store); CTAS is the occupancy the launch bounds aim for.
+template <int COLS, bool SEP, int CTAS>
+struct PencilShape {
+    static constexpr int cols = COLS, threads = 32 * COLS, ctas = CTAS;
+    static constexpr bool sep = SEP;
+};
+using PencilZ = PencilShape<8, false, 2>;   // 64-byte pieces of B rows
+using PencilY = PencilShape<4, true, 3>;    // 32-byte pieces of C rows
 
-// row-major column of 33 T slots (km_slot), padded so that 8 columns start 2 banks apart
-template <int T>
+// row-major column of 33 T slots (km_slot), padded so that the COLS columns of a CTA
+// start 32 / COLS banks apart (conflict-free transposed reads, 64-bit accesses)
+template <int T, int COLS>
 __host__ __device__ constexpr int pencil_stride() {
-    return 33 * T + (((2 - 33 * T) % 16) + 16) % 16;
+    return 33 * T + (((16 / COLS - 33 * T) % 16) + 16) % 16;
 }
 
-// Z / Y shared memory: one slot of 8 columns, the bulk-copy destination (stride N) and
-// then the row-major outputs (stride S >= N)
-template <int T>
+// Z / Y shared memory: the bulk-copy destination (COLS columns of N), then the row-major
+// outputs (COLS columns of S) after it or over it
+template <int T, class Sh>
 constexpr size_t pencil_smem_yz() {
-    return (size_t)kPencilCols * pencil_stride<T>() * sizeof(float2);
+    return (size_t)Sh::cols * ((Sh::sep ? 32 * T : 0) + pencil_stride<T, Sh::cols>()) *
+           sizeof(float2);
 }
 
 // C rows hold the n/2 + 1 modes of one (z, y) padded to a multiple of 16 complex values
@@ -613,7 +628,7 @@ __host__ __device__ constexpr int pencil_rows() {
 // pencil_rows already finished across lanes (y[k2 + T bitrev5(lane)]): it writes every row
 // k2 to slots k2 * 33 + (lane or k1), the CTA finishes the remaining 32-point row DFTs one
 // per thread, and dst[r * pitch + c] = column c's output lo + r for r < R, c < ncol.
-template <int T, int S>
+template <int T, int S, int COLS>
 __device__ __forceinline__ void pencil_finish(float2* __restrict__ ob,
                                               const htfft::C2 (&v)[T], float2* dst,
                                               long long pitch, int lo, int R, int ncol,
@@ -628,26 +643,27 @@ __device__ __forceinline__ void pencil_finish(float2* __restrict__ ob,
         for (int k2 = TB; k2 < T; ++k2) ob[w * S + k2 * 33 + k1] = make_float2(v[k2].x, v[k2].y);
     }
     __syncthreads();
-    for (int j = tid; j < ncol * TB; j += 256) {
+    for (int j = tid; j < ncol * TB; j += 32 * COLS) {
         const int c = j / TB, k2 = j - c * TB;
         htfft::dft32_row(ob + c * S + k2 * 33);
     }
     __syncthreads();
-    for (int e = tid; e < kPencilCols * R; e += 256) {
-        const int r = e >> 3, c = e & 7;
+    for (int e = tid; e < COLS * R; e += 32 * COLS) {
+        const int r = e / COLS, c = e % COLS;
         if (c < ncol) dst[(long long)r * pitch + c] = ob[c * S + htfft::km_slot<T>(lo + r)];
     }
 }
 
-template <int T>
-__global__ void __launch_bounds__(256, 2) pz_kernel(
+template <int T, class Sh>
+__global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     const float2* __restrict__ P, float2* __restrict__ B, int NK, int zlo, int Rz,
     const float* __restrict__ tab, const float2* __restrict__ twL,
     const float2* __restrict__ tw32, int32_t* __restrict__ status) {
-    constexpr int N = 32 * T, S = pencil_stride<T>(), NB = N / kPencilCols, H = T / 2;
+    constexpr int COLS = Sh::cols, N = 32 * T, S = pencil_stride<T, COLS>(), NB = N / COLS,
+                  H = T / 2;
     extern __shared__ __align__(128) float2 sm[];
-    float2* in = sm;                          // 8 input columns of N
-    float2* ob = sm;                          // then 8 row-major columns of S
+    float2* in = sm;                          // the input columns, N each
+    float2* ob = Sh::sep ? sm + COLS * N : sm;   // the row-major columns, S each
     __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int ntasks = NK * NB;               // task = kx * NB + ky block
@@ -657,9 +673,9 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(
     }
     __syncthreads();
     auto issue = [&](int tk) {                // thread 0
-        const int kx = tk / NB, ky0 = (tk - kx * NB) * kPencilCols;
-        htasync::bar_expect(&bar, kPencilCols * N * (unsigned)sizeof(float2));
-        for (int c = 0; c < kPencilCols; ++c)
+        const int kx = tk / NB, ky0 = (tk - kx * NB) * COLS;
+        htasync::bar_expect(&bar, COLS * N * (unsigned)sizeof(float2));
+        for (int c = 0; c < COLS; ++c)
             htasync::bulk_load(in + c * N, P + ((long long)(ky0 + c) * NK + kx) * N,
                                N * (unsigned)sizeof(float2), &bar);
     };
@@ -670,7 +686,7 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(
     unsigned parity = 0;
     bool ok = true;
     for (; task < ntasks; task += gridDim.x) {
-        const int kx = task / NB, ky0 = (task - kx * NB) * kPencilCols, ky = ky0 + w;
+        const int kx = task / NB, ky0 = (task - kx * NB) * COLS, ky = ky0 + w;
         // Window W(base + sz^2), gathered before the wait (scattered L2 reads that do not
         // depend on the copy).  Each value is fetched once: kz = lane + 32 t < N/2 for
         // t < H; the upper half kz' = N - kz (same sz^2) is lane 32 - lane's value at
@@ -695,7 +711,11 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(
         const float2* col = in + w * N;
 #pragma unroll
         for (int t = 0; t < T; ++t) v[t] = htfft::to_c2(col[lane + 32 * t]);
-        __syncthreads();                      // every column is in registers: reuse the slot
+        __syncthreads();                      // every column is in registers
+        if (Sh::sep && tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
 #pragma unroll
         for (int t = 0; t < T; ++t) {
             float wv;
@@ -711,12 +731,16 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(
         }
         htfft::warp_ifft_inner<T>(v, twL, lane);
         htfft::cross32<T, pencil_rows<T>()>(v, lane, w32);
-        pencil_finish<T, S>(ob, v, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, kPencilCols,
-                            tid);
-        __syncthreads();
-        if (tid == 0 && task + (int)gridDim.x < ntasks) {
-            htasync::fence_async_smem();
-            issue(task + (int)gridDim.x);
+        pencil_finish<T, S, COLS>(ob, v, B + (long long)kx * Rz * N + ky0, N, zlo, Rz, COLS,
+                                  tid);
+        // with a separate slot the barrier at the top of the next item orders these reads
+        // of ob before its writes; else the slot is refilled once every thread is done
+        if (!Sh::sep) {
+            __syncthreads();
+            if (tid == 0 && task + (int)gridDim.x < ntasks) {
+                htasync::fence_async_smem();
+                issue(task + (int)gridDim.x);
+            }
         }
     }
     if (!ok && tid == 0) {
@@ -726,18 +750,18 @@ __global__ void __launch_bounds__(256, 2) pz_kernel(
     }
 }
 
-template <int T>
-__global__ void __launch_bounds__(256, 2) py_kernel(
+template <int T, class Sh>
+__global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
     const float2* __restrict__ B, float2* __restrict__ C, int NK, int NKP, int Rz, int ylo,
     int Ry, const float2* __restrict__ twL, const float2* __restrict__ tw32,
     int32_t* __restrict__ status) {
-    constexpr int N = 32 * T, S = pencil_stride<T>();
+    constexpr int COLS = Sh::cols, N = 32 * T, S = pencil_stride<T, COLS>();
     extern __shared__ __align__(128) float2 sm[];
     float2* in = sm;
-    float2* ob = sm;
+    float2* ob = Sh::sep ? sm + COLS * N : sm;
     __shared__ __align__(8) unsigned long long bar;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int NKB = (NK + kPencilCols - 1) / kPencilCols;
+    const int NKB = (NK + COLS - 1) / COLS;
     const int ntasks = Rz * NKB;              // task = zr * NKB + kx block
     if (tid == 0) {
         htasync::bar_init(&bar, 1);
@@ -745,8 +769,8 @@ __global__ void __launch_bounds__(256, 2) py_kernel(
     }
     __syncthreads();
     auto issue = [&](int tk) {                // thread 0
-        const int zr = tk / NKB, kx0 = (tk - zr * NKB) * kPencilCols;
-        const int ncol = min(kPencilCols, NK - kx0);
+        const int zr = tk / NKB, kx0 = (tk - zr * NKB) * COLS;
+        const int ncol = min(COLS, NK - kx0);
         htasync::bar_expect(&bar, ncol * N * (unsigned)sizeof(float2));
         for (int c = 0; c < ncol; ++c)
             htasync::bulk_load(in + c * N, B + ((long long)(kx0 + c) * Rz + zr) * N,
@@ -759,8 +783,8 @@ __global__ void __launch_bounds__(256, 2) py_kernel(
     unsigned parity = 0;
     bool ok = true;
     for (; task < ntasks; task += gridDim.x) {
-        const int zr = task / NKB, kx0 = (task - zr * NKB) * kPencilCols;
-        const int ncol = min(kPencilCols, NK - kx0);
+        const int zr = task / NKB, kx0 = (task - zr * NKB) * COLS;
+        const int ncol = min(COLS, NK - kx0);
         ok = tid == 0 ? htasync::bar_wait(&bar, parity) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
@@ -773,16 +797,23 @@ __global__ void __launch_bounds__(256, 2) py_kernel(
 #pragma unroll
             for (int t = 0; t < T; ++t) v[t] = htfft::to_c2(col[lane + 32 * t]);
         }
-        __syncthreads();
+        __syncthreads();                      // the columns are in registers
+        if (Sh::sep && tid == 0 && task + (int)gridDim.x < ntasks) {
+            htasync::fence_async_smem();
+            issue(task + (int)gridDim.x);
+        }
         if (w < ncol) {   // warp-uniform
             htfft::warp_ifft_inner<T>(v, twL, lane);
             htfft::cross32<T, pencil_rows<T>()>(v, lane, w32);
         }
-        pencil_finish<T, S>(ob, v, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry, ncol, tid);
-        __syncthreads();
-        if (tid == 0 && task + (int)gridDim.x < ntasks) {
-            htasync::fence_async_smem();
-            issue(task + (int)gridDim.x);
+        pencil_finish<T, S, COLS>(ob, v, C + (long long)zr * Ry * NKP + kx0, NKP, ylo, Ry,
+                                  ncol, tid);
+        if (!Sh::sep) {
+            __syncthreads();
+            if (tid == 0 && task + (int)gridDim.x < ntasks) {
+                htasync::fence_async_smem();
+                issue(task + (int)gridDim.x);
+            }
         }
     }
     if (!ok && tid == 0) {
@@ -896,29 +927,30 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
                          int zlo, int zhi, int ylo, int yhi, cudaStream_t st) {
     constexpr int n = 32 * T, TH = T / 2;
     const int nk = n / 2 + 1, nkp = pencil_row_pitch(n), Rz = zhi - zlo, Ry = yhi - ylo;
-    const size_t smyz = pencil_smem_yz<T>(), smx = pencil_smem_x<TH>();
-    HT_CUDA_TRY(cudaFuncSetAttribute(pz_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "pz smem");
-    HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smyz), "py smem");
+    const size_t smz = pencil_smem_yz<T, PencilZ>(), smy = pencil_smem_yz<T, PencilY>(),
+                 smx = pencil_smem_x<TH>();
+    HT_CUDA_TRY(cudaFuncSetAttribute(pz_kernel<T, PencilZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smz), "pz smem");
+    HT_CUDA_TRY(cudaFuncSetAttribute(py_kernel<T, PencilY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smy), "py smem");
     HT_CUDA_TRY(cudaFuncSetAttribute(px_kernel<TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx), "px smem");
     int bz = 0, by = 0, bx = 0;
-    constexpr int nty = 256;
-    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bz, pz_kernel<T>, nty, smyz), "pz occupancy");
-    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, py_kernel<T>, nty, smyz), "py occupancy");
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bz, pz_kernel<T, PencilZ>, PencilZ::threads, smz), "pz occupancy");
+    HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&by, py_kernel<T, PencilY>, PencilY::threads, smy), "py occupancy");
     HT_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bx, px_kernel<TH>, 256, smx), "px occupancy");
     if (bz < 1 || by < 1 || bx < 1) return ht_fail(HT_ERR_CUDA, "pencil kernels do not fit an SM");
     const FusedTw tw = fused_tw(ctx, n);
     int32_t* status = ht_status_word(ctx);
     const long long sms = ctx->num_sms;
-    const long long zt = (long long)nk * (n / kPencilCols);
-    const long long yt = (long long)Rz * ((nk + kPencilCols - 1) / kPencilCols);
+    const long long zt = (long long)nk * (n / PencilZ::cols);
+    const long long yt = (long long)Rz * ((nk + PencilY::cols - 1) / PencilY::cols);
     const long long rows = (long long)Rz * Ry;
     const unsigned gz = (unsigned)std::min(zt, sms * bz);
     const unsigned gy = (unsigned)std::min(yt, sms * by);
     const unsigned gx = (unsigned)std::min((rows + 7) / 8, sms * bx);
-    pz_kernel<T><<<gz, nty, smyz, st>>>(P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL,
-                                        tw.w32, status);
+    pz_kernel<T, PencilZ><<<gz, PencilZ::threads, smz, st>>>(
+        P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL, tw.w32, status);
     HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
-    py_kernel<T><<<gy, nty, smyz, st>>>(B, C, nk, nkp, Rz, ylo, Ry, tw.lmL, tw.w32, status);
+    py_kernel<T, PencilY><<<gy, PencilY::threads, smy, st>>>(B, C, nk, nkp, Rz, ylo, Ry,
+                                                             tw.lmL, tw.w32, status);
     HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
     px_kernel<TH><<<gx, 256, smx, st>>>(C, d_out, nkp, zlo, ylo, Ry, rows, tw.nat, tw.lmM,
                                         tw.w32, status);
