@@ -1,7 +1,7 @@
 """Benchmark of the halo-finding hot path: peak finding + radial-shell collapse.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tile1152|box512|box128] [--mode batched|plain]
+                    [--workload tile1152|box512|box128|collapse_table] [--mode batched|plain]
 
 Metric: candidate peaks per second carried through peak finding (all filters, mask
 carried) and the radial-shell collapse, for one tile per GPU (weak scaling: N GPUs run N
@@ -16,6 +16,11 @@ Inputs are seeded synthetic fields (BBKS LambdaCDM, Threefry noise, 2LPT), gener
 the device before timing; they are far larger than the 126 MB L2, so no flush is needed.
 `--impl reference` times the CPU oracle (the C restatement of RadialShell.analyse_peak
 and PeakFind.find_peaks) on the host cores on a bounded sample of the same workload.
+
+`--workload collapse_table` measures the collapse-table generator instead (metric:
+ellipsoids per second through the RK4 collapse, EllipsoidalCollapse.jl:492-590): a step
+is the default 50 x 20 x 20 table (CollapseTable.jl:29-76) at the generator's default
+cosmology, 20,000 independent ellipsoids, one per device thread.
 """
 from __future__ import annotations
 
@@ -615,13 +620,118 @@ def run_reference(args, rank, world, device):
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+COLLAPSE_METRIC = "ellipsoids/s thru RK4 collapse-table generation"
+
+
+def _collapse_setup(ht):
+    col, cat = ht.collapse, ht.catalog
+    cp = cat.CosmologyParams(Om=0.315, OB=0.049, OL=0.685, h=0.674, ns=0.965, s8=0.808)
+    ep = col.EllipsoidParams(cp)
+    tp = col.CollapseTableParams()
+    return cp, ep, tp
+
+
+def _collapse_cpu(ep, tp):
+    """The oracle's make_table (C restatement, OpenMP on every host thread), once."""
+    from oracle import collapse as oc, max_threads
+    eo = oc.EllipsoidOracle(ep.dlin_tables, ep.cosmo.Om, ep.cosmo.OL)
+    t0 = time.perf_counter()
+    eo.make_table(tp.Nx, tp.Ny, tp.Nz, *tp.axes)
+    dt = time.perf_counter() - t0
+    n = tp.Nx * tp.Ny * tp.Nz
+    return {"value": n / dt, "unit": "ellipsoids/s", "cores": max_threads(), "kind": "port",
+            "sample": f"the whole {tp.Nx}x{tp.Ny}x{tp.Nz} table ({n} ellipsoids), or_make_table "
+                      f"(C restatement of the RK4 path, FP64, OpenMP)"}
+
+
+def run_collapse_table(args, rank, world, device):
+    """The collapse-table row: every rank builds the default table (replicas: the table
+    is one small offline input).  value = ellipsoids per second of the device kernel over
+    K launches (CUDA events on the launching stream, max over ranks); e2e = the host API
+    ht_collapse_table (grid upload, launch, table download) timed around each call."""
+    import torch
+    ht = _package()
+    cp, ep, tp = _collapse_setup(ht)
+    n = tp.Nx * tp.Ny * tp.Nz
+    config = {"workload": "collapse_table",
+              "desc": f"{tp.Nx}x{tp.Ny}x{tp.Nz} zvir table (log10 Frho, e_v, p_v/e_v), "
+                      "RK4 tfac 0.01, nstepmax 10000, Planck 2018 (Om 0.315, OL 0.685)",
+              "ellipsoids_per_step": n, "l2": "inputs 480 KB: compute bound, no flush",
+              "parallelism": f"replicas x{world}"}
+    if args.impl == "reference":
+        if rank != 0:
+            return None
+        vals = [_collapse_cpu(ep, tp) for _ in range(args.warmup + args.steps)][args.warmup:]
+        v = float(np.mean([c["value"] for c in vals]))
+        cb = dict(vals[-1])
+        cb["value"] = v
+        return {"metric": COLLAPSE_METRIC, "value": v, "unit": "ellipsoids/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (the table's own grid)", "config": config,
+                "impl": "reference", "cpu_baseline": cb,
+                "e2e": {"value": v, "unit": "ellipsoids/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+    X1, X2, Y1, Y2, Z1, Z2 = tp.axes
+    q = np.arange(n)
+    i, j, k = q % tp.Nx, (q // tp.Nx) % tp.Ny, q // (tp.Nx * tp.Ny)
+    x = X1 + i * ((X2 - X1) / (tp.Nx - 1))
+    y = Y1 + j * ((Y2 - Y1) / (tp.Ny - 1))
+    z = Z1 + k * ((Z2 - Z1) / (tp.Nz - 1))
+    F = torch.tensor(np.power(10.0, x), dtype=torch.float64, device=device)
+    E = torch.tensor(y, dtype=torch.float64, device=device)
+    P = torch.tensor(z * y, dtype=torch.float64, device=device)
+    for _ in range(args.warmup):
+        ht.collapse.evolve_ellipses(F, E, P, ep, device=device.index or 0)
+    torch.cuda.synchronize()
+    clocks = Clocks(device.index or 0) if rank == 0 else None
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        ht.collapse.evolve_ellipses(F, E, P, ep, device=device.index or 0)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=device)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    ck = clocks.stop() if clocks else None
+    # end to end through the host API (grid upload, launch, table download)
+    wall = []
+    for _ in range(max(args.steps, 1)):
+        t0 = time.perf_counter()
+        ht.collapse.make_table(ep, tp, device=device.index or 0)
+        wall.append(time.perf_counter() - t0)
+    e2e_s = float(np.median(wall))
+    ntab = len(ep.dlin_tables.atab)
+    line = {"metric": COLLAPSE_METRIC, "value": world * n / (ms / 1e3), "unit": "ellipsoids/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the table's own grid)", "config": config,
+            "roofline": None,
+            "roofline_note": "latency-bound FP64 chains (one ellipsoid per thread, ~10^3 "
+                             "dependent RK4 steps); no HBM or tensor-core bound applies",
+            "gpu_launches": args.steps, "clocks": ck,
+            "e2e": {"value": world * n / e2e_s, "unit": "ellipsoids/s",
+                    "h2d_bytes_per_step": 3 * n * 8 + 3 * ntab * 8,
+                    "d2h_bytes_per_step": n * 8, "ms_per_step": 1e3 * e2e_s}}
+    if rank == 0 and world == 1 and args.cpu_seconds > 0:
+        line["cpu_baseline"] = _collapse_cpu(ep, tp)
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tile1152", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="tile1152",
+                    choices=list(WORKLOADS) + ["collapse_table"])
     ap.add_argument("--mode", default="learned", choices=["learned", "batched", "plain"])
     ap.add_argument("--graph", type=int, default=1,
                     help="capture the per-filter smoothing + peak-scan loop in a CUDA graph")
@@ -644,7 +754,9 @@ def main():
                                              device_id=torch.device("cuda", local))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
-    if args.impl == "reference":
+    if args.workload == "collapse_table":
+        line = run_collapse_table(args, rank, world, device)
+    elif args.impl == "reference":
         line = run_reference(args, rank, world, device)
     else:
         line = run_ours(args, rank, world, device)

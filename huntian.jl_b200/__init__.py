@@ -9,7 +9,7 @@ from ._lib import (HT_CONV_CPU, HT_CONV_GPU, HT_MODE_BATCHED, HT_MODE_PLAIN, HTE
 from .host import (HaloFinder, PeakCandidate, analyse_peaks_gpu_cuda_multirf, ir2min_of,
                    nhunt_of, peak_find_tile_gpu)
 from .tables import log_filterbank, read_filterbank, read_homeltab, write_homeltab
-from . import bracket, catalog, dist
+from . import bracket, catalog, collapse, dist
 
 __all__ = ["HaloFinder", "PeakCandidate", "peak_find_tile_gpu",
            "analyse_peaks_gpu_cuda_multirf", "ir2min_of",

@@ -42,7 +42,8 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
            "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
            "ht_bracket_adam", "ht_ctx_tune", "ht_ctx_set_cosmo", "ht_peak_lightcone",
-           "ht_pack_halos", "ht_merge_halos", "ht_finalize_eulerian")
+           "ht_pack_halos", "ht_merge_halos", "ht_finalize_eulerian", "ht_evolve_ellipses",
+           "ht_collapse_table")
 
 
 class HTError(RuntimeError):
@@ -91,6 +92,18 @@ class HtCosmo(C.Structure):
                 ("atab", _P), ("D_atab", _P), ("dlnD_dlna", _P), ("ntab", C.c_int32)] + \
         [(n, C.c_double) for n in ("amintab", "amaxtab", "D_ainfty", "D_a0", "HD_Hainfty",
                                    "HD_Ha0", "Om", "OL")]
+
+
+class HtEllipsoid(C.Structure):
+    _fields_ = [("Om", C.c_double), ("OL", C.c_double), ("iforce_strat", C.c_int32),
+                ("ivir_strat", C.c_int32), ("fcoll", C.c_double * 3), ("tfac", C.c_double),
+                ("nstepmax", C.c_int32), ("zinit_fac", C.c_double)]
+
+
+class HtGrowth(C.Structure):
+    _fields_ = [("atab", _P), ("D_atab", _P), ("dlnD_dlnatab", _P), ("ntab", C.c_int32)] + \
+        [(n, C.c_double) for n in ("amintab", "amaxtab", "D_ainfty", "D_a0", "HD_Hainfty",
+                                   "HD_Ha0")]
 
 
 class HtTileGeom(C.Structure):
@@ -187,6 +200,12 @@ def load() -> C.CDLL:
     L.ht_merge_halos.argtypes = [_P, _P, i64, i32, i32, i32, _P, _P, _P]
     L.ht_finalize_eulerian.restype = C.c_int
     L.ht_finalize_eulerian.argtypes = [_P, _P, i64, i32, _P, i32, dbl, _P]
+    L.ht_evolve_ellipses.restype = C.c_int
+    L.ht_evolve_ellipses.argtypes = [C.c_int, C.POINTER(HtEllipsoid), C.POINTER(HtGrowth), i64,
+                                     _P, _P, _P, i32, _P, _P, _P, _P, _P]
+    L.ht_collapse_table.restype = C.c_int
+    L.ht_collapse_table.argtypes = [C.c_int, C.POINTER(HtEllipsoid), C.POINTER(HtGrowth), i32,
+                                    i32, i32] + [dbl] * 6 + [_P]
     _lib = L
     return L
 

@@ -4,7 +4,10 @@
 
 Compiles every .cu under csrc/ with nvcc for sm_100a only (no fast-math: the collapse
 criterion needs IEEE divisions, square roots and NaN propagation) and links them into
-one shared library with a plain C ABI (include/huntian_b200.h).  --smallcase also builds
+one shared library with a plain C ABI (include/huntian_b200.h).  The files listed in
+FILE_FLAGS are compiled to objects of their own with extra flags first (ht_collapse.cu
+with -fmad=false: the ellipsoid integration keeps every product unfused, as the
+reference's Julia arithmetic does).  --smallcase also builds
 pencil_smallcase, the reduced-size driver of the 1152^3 pencil smoothing kernels used for
 ncu captures.
 """
@@ -22,8 +25,31 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
          "-cudart", "shared", "-I", os.path.join(ROOT, "include"), "-lcufft"]
 
 
+FILE_FLAGS = {"ht_collapse.cu": ["-fmad=false"]}
+OBJDIR = os.path.join(HERE, "_build")
+
+
 def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+
+
+def _split_sources(srcs):
+    plain = [f for f in srcs if os.path.basename(f) not in FILE_FLAGS]
+    special = [f for f in srcs if os.path.basename(f) in FILE_FLAGS]
+    return plain, special
+
+
+def _objects(special, flags):
+    """Compile the FILE_FLAGS sources to position-independent objects."""
+    os.makedirs(OBJDIR, exist_ok=True)
+    objs = []
+    base = [f for f in flags if f not in ("-shared", "-cudart", "shared", "-lcufft", "-lcuda")]
+    for src in special:
+        obj = os.path.join(OBJDIR, os.path.basename(src)[:-3] + ".o")
+        subprocess.run([NVCC] + base + FILE_FLAGS[os.path.basename(src)] +
+                       ["-Xcompiler", "-fPIC", "-c", src, "-o", obj], check=True)
+        objs.append(obj)
+    return objs
 
 
 def deps():
@@ -40,7 +66,10 @@ def needs_build() -> bool:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or needs_build():
-        cmd = [NVCC] + FLAGS + (["-Xptxas", "-v"] if verbose else []) + sources() + ["-o", LIB]
+        plain, special = _split_sources(sources())
+        extra = ["-Xptxas", "-v"] if verbose else []
+        objs = _objects(special, FLAGS + extra)
+        cmd = [NVCC] + FLAGS + extra + plain + objs + ["-o", LIB]
         subprocess.run(cmd, check=True)
     return LIB
 
@@ -49,10 +78,12 @@ def build_smallcase() -> str:
     """pencil_smallcase: pencil_smallcase.cu (which includes csrc/ht_smooth.cu) linked with
     the other sources."""
     out = os.path.join(HERE, "pencil_smallcase")
-    srcs = [os.path.join(HERE, "pencil_smallcase.cu")] + \
-        [f for f in sources() if os.path.basename(f) != "ht_smooth.cu"]
+    plain, special = _split_sources([f for f in sources()
+                                     if os.path.basename(f) != "ht_smooth.cu"])
+    objs = _objects(special, FLAGS)
+    srcs = [os.path.join(HERE, "pencil_smallcase.cu")] + plain
     flags = [f for f in FLAGS if f not in ("-shared", "-Xcompiler", "-fPIC", "-fvisibility=hidden")]
-    subprocess.run([NVCC] + flags + ["-lcuda"] + srcs + ["-o", out], check=True)
+    subprocess.run([NVCC] + flags + ["-lcuda"] + srcs + objs + ["-o", out], check=True)
     return out
 
 

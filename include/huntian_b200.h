@@ -40,6 +40,10 @@
  *   ht_finalize_eulerian -> src/Merger/Merger.jl:114-146 `finalize_eulerian`
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
+ *   ht_evolve_ellipses  -> src/EllipsoidalCollapse/EllipsoidalCollapse.jl:492-590
+ *                          `evolve_ellipse_full` (solver = :rk4), many ellipsoids at once
+ *   ht_collapse_table   -> src/EllipsoidalCollapse/CollapseTable.jl:29-76 `make_table` /
+ *                          `make_table_threaded` (bin/generate_table.jl --solver rk4)
  */
 #ifndef HUNTIAN_B200_H
 #define HUNTIAN_B200_H
@@ -459,6 +463,51 @@ HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* sh
  * of the peak scan gave up after 2 s (that filter's peaks are then incomplete); the word
  * is cleared on read. */
 HT_API int ht_device_status(ht_ctx* ctx, int32_t* status);
+
+/* ---------------------------------------------------- collapse-table generation ---- */
+
+/* EllipsoidParams (src/EllipsoidalCollapse/EllipsoidalCollapse.jl:10-45) with its
+ * cosmology's Om and OL; the defaults there are iforce_strat 4, ivir_strat 2, fcoll
+ * (0.01, 0.171, 0.171), tfac 0.01, nstepmax 10000, zinit_fac 20. */
+typedef struct {
+    double Om, OL;
+    int32_t iforce_strat;     /* 0, 1, 3, 4, 5 or 6 (2 leaves the velocities constant) */
+    int32_t ivir_strat;       /* 1 or 2 */
+    double fcoll[3];          /* fcoll_1, fcoll_2, fcoll_3 */
+    double tfac;              /* RK4 step factor */
+    int32_t nstepmax;         /* step limit, 1 .. 10^8 */
+    double zinit_fac;         /* initial 1/a = zinit_fac Frho */
+} ht_ellipsoid;
+
+/* DlinearTables (src/Cosmology/Cosmology.jl:68-78), HOST arrays of ntab >= 4 entries, atab
+ * ascending (as Dlinear_tables builds it). */
+typedef struct {
+    const double* atab;
+    const double* D_atab;        /* D(a) / a */
+    const double* dlnD_dlnatab;
+    int32_t ntab;
+    double amintab, amaxtab, D_ainfty, D_a0, HD_Hainfty, HD_Ha0;
+} ht_growth;
+
+/* evolve_ellipse_full with the fixed-step RK4 (EllipsoidalCollapse.jl:492-590) for n
+ * ellipsoids (DEVICE arrays Frho, e_v, p_v), event idynax (1-3 axis virialisation, 4-6
+ * turnaround): d_zvir = 1/a at the event, d_D = D(a) there, d_fc = Frho D, all -1 when the
+ * event does not happen before a = 2 or nstepmax steps.  d_D, d_fc and d_steps (steps
+ * taken) may be NULL.  One device thread per ellipsoid, FP64.  Asynchronous on `stream`
+ * (the growth table is staged to the device in stream order; the host arrays may be
+ * released when the call returns). */
+HT_API int ht_evolve_ellipses(int device, const ht_ellipsoid* ep, const ht_growth* growth,
+                              int64_t n, const double* d_Frho, const double* d_e_v,
+                              const double* d_p_v, int32_t idynax, double* d_zvir,
+                              double* d_D, double* d_fc, int32_t* d_steps, void* stream);
+
+/* make_table (CollapseTable.jl:29-50): table[i, j, k] = Float32(zvir) of the ellipsoid
+ * Frho = 10^x_i, e_v = y_j, p_v = z_k y_j on the regular axes x_i = X1 + (i - 1)(X2 - X1) /
+ * (nx - 1) and so on (event 1, axis-1 virialisation), written column-major (i fastest)
+ * into the HOST array table[nx ny nz].  Synchronous. */
+HT_API int ht_collapse_table(int device, const ht_ellipsoid* ep, const ht_growth* growth,
+                             int32_t nx, int32_t ny, int32_t nz, double X1, double X2,
+                             double Y1, double Y2, double Z1, double Z2, float* table);
 
 #ifdef __cplusplus
 }

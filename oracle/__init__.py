@@ -25,7 +25,7 @@ def build(force: bool = False) -> str:
     """Compile liboracle.so with the Makefile beside this file."""
     if force or not os.path.exists(_LIB_PATH) or (
         os.path.getmtime(_LIB_PATH) < max(os.path.getmtime(os.path.join(_HERE, f))
-                                           for f in ("ht_oracle.c", "ht_oracle.h"))):
+                                           for f in ("ht_oracle.c", "or_collapse.c", "ht_oracle.h"))):
         subprocess.run(["make", "-s", "-C", _HERE, "-B", "liboracle.so"], check=True)
     return _LIB_PATH
 

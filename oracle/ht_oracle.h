@@ -97,6 +97,34 @@ void or_analyse_batch(const or_grid* g, int64_t npeaks, const int32_t* pi, const
 
 int or_max_threads(void);
 
+/* ---- collapse-table generation (or_collapse.c) ---- */
+
+/* DlinearTables (Cosmology.jl:68-78): D(a)/a and dlnD/dlna on an ascending table of a. */
+typedef struct {
+    const double* atab; const double* D_atab; const double* dlnD; int ntab;
+    double amintab, amaxtab, D_ainfty, D_a0, HD_Hainfty, HD_Ha0;
+} or_growth;
+
+/* EllipsoidParams (EllipsoidalCollapse.jl:10-45) with its cosmology (Om, OL). */
+typedef struct {
+    double Om, OL;
+    int iforce_strat, ivir_strat;
+    double fcoll[3];          /* fcoll_1, fcoll_2, fcoll_3 */
+    double tfac;
+    int nstepmax;
+    double zinit_fac;
+    or_growth growth;
+} or_ellipsoid;
+
+void   or_dlinear_ab(const or_growth* g, double ai, double* dlin, double* hd_ha);
+double or_dfnofa(const or_growth* g, double ai);
+double or_elliptic_rd(double x, double y, double z);
+void   or_get_b_2(double a1, double a2, double a3, double b[3]);
+int    or_evolve_ellipse(const or_ellipsoid* ep, double Frho, double e_v, double p_v,
+                         int idynax, double out[3]);
+void   or_make_table(const or_ellipsoid* ep, int nx, int ny, int nz, double X1, double X2,
+                     double Y1, double Y2, double Z1, double Z2, float* table);
+
 #ifdef __cplusplus
 }
 #endif
