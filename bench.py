@@ -250,11 +250,17 @@ class Workload:
             self.pf_loop()
         torch.cuda.synchronize()
 
-    def step(self, ev=None, fields_ready=None):
+    def step(self, ev=None, fields_ready=None, hooks=None):
         """One tile: peak scan over all filters, then pack + shell collapse.  fields_ready:
         an event after which the six displacement fields are on the device (they are first
-        read by the pack, so their host copies may overlap the peak finding)."""
+        read by the pack, so their host copies may overlap the peak finding).  hooks: optional
+        callables run on the host at the stage boundaries, where the end-to-end pipeline
+        orders its copies: "start" (before the first write), "graph" (npk; the peaks are
+        final), "pack" (delta and the displacement fields have been read), "walk" (before the
+        walk writes the results and the mask), "end" (npk; results, mask, halos final)."""
         import torch
+        call = lambda name, *a: hooks[name](*a) if hooks and name in hooks else None
+        call("start")
         self.mask.zero_()
         self.peaks["count"].zero_()
         self.peaks["found"].zero_()
@@ -275,6 +281,7 @@ class Workload:
             self.dk = None
         npk = int(self.peaks["count"].item())
         self.npeaks = npk
+        call("graph", npk)
         self.mask.zero_()                                # MultiResolution.jl:1083
         t = self.tile
         if ev is not None:
@@ -283,6 +290,7 @@ class Workload:
             torch.cuda.current_stream().wait_event(fields_ready)
         self.finder.bind_fields(t["delta"], t["etax"], t["etay"], t["etaz"], t["eta2x"],
                                 t["eta2y"], t["eta2z"], None)
+        call("pack")
         if ev is not None:
             ev["pack"][1].record()
         fidx = self.peaks["filter_idx"][:npk].long() - 1
@@ -290,6 +298,7 @@ class Workload:
         ir2 = self.ir2_f[fidx]
         zz = torch.full((npk,), self.ZZon, dtype=torch.float32, device=self.device)
         fc = torch.full((npk,), self.fcrit, dtype=torch.float32, device=self.device)
+        call("walk")
         if self.results is None or self.results["RTHL"].numel() < npk:
             self.results = self.ht.HaloFinder.alloc_results(npk, self.device)
         pi, pj, pk = self.peaks["i"][:npk], self.peaks["j"][:npk], self.peaks["k"][:npk]
@@ -314,6 +323,7 @@ class Workload:
                                                 ilpt=2, ioutshear=0)
         if ev is not None and "records" in ev:
             ev["records"][1].record()
+        call("end", npk)
         return npk
 
     def time_walk(self, reps=2):
@@ -455,11 +465,17 @@ def run_ours(args, rank, world, device):
 
 
 def run_e2e(ht, W, args):
-    """Same step through the public host-buffer API: fields start in pinned host memory and
-    are copied into the device tile inside the timed region, and all results (peaks, the 14
-    result arrays, the mask and the halo records) are read back into pinned host buffers.  delta is copied
-    first; the six displacement fields, first needed by the pack, copy on a second stream
-    while the peak finding runs."""
+    """Same step through the public host-buffer API, K steps back to back: every step's
+    fields start in pinned host memory and are copied into the device tile inside the timed
+    region, and all of its results (peaks, the 14 result arrays, the mask and the halo
+    records) are read back into pinned host buffers inside it.  The copies run on two copy
+    streams beside the compute, ordered by events as a tile pipeline would: step s + 1's
+    delta and displacement fields go up once step s's pack has read the tile (during step
+    s's walk and step s + 1's peak finding; the pack of s + 1 waits for them), step s's
+    peaks come down during its walk, and its results, mask (copied on the device into a
+    read-back buffer first: the next step clears the mask the peak scan uses) and halo
+    records during step s + 1's peak finding (the walk of s + 1 waits for them).  Only the
+    first step's delta upload and the last step's read-back are not overlapped."""
     import torch
     host = {k: v.cpu().pin_memory() for k, v in W.tile.items()}
     h2d = sum(t.numel() * t.element_size() for t in host.values())
@@ -473,58 +489,106 @@ def run_e2e(ht, W, args):
                 .pin_memory() for g, n in names}
     out_host["mask"] = torch.empty(W.mask.shape, dtype=W.mask.dtype).pin_memory()
     out_host["halos"] = torch.empty(W.halos.numel(), dtype=torch.float32).pin_memory()
-    side = torch.cuda.Stream()
+    mask_out = torch.empty_like(W.mask)
     main = torch.cuda.current_stream()
-    d2h = 0
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
     mk = lambda: torch.cuda.Event(enable_timing=True)
-    s0, s1 = mk(), mk()
-    parts = {"h2d_delta": 0.0, "step": 0.0, "d2h": 0.0}
-    s0.record()
-    tot = 0
-    for _ in range(args.e2e_steps):
-        e = [mk() for _ in range(4)]
-        e[0].record()
-        W.tile["delta"].copy_(host["delta"], non_blocking=True)   # into the device tile
-        e[1].record()
-        side.wait_stream(main)
-        with torch.cuda.stream(side):
+    K = max(1, args.e2e_steps)
+    st = {"d2h": 0, "tot": 0, "peaks_done": None, "res_done": None}
+
+    def upload():
+        """delta, then the six displacement fields, on the upload stream."""
+        with torch.cuda.stream(up):
+            W.tile["delta"].copy_(host["delta"], non_blocking=True)
+            d = torch.cuda.Event()
+            d.record(up)
             for k, v in host.items():
                 if k != "delta":
                     W.tile[k].copy_(v, non_blocking=True)
-            ready = torch.cuda.Event()
-            ready.record(side)
-        npk = W.step(fields_ready=ready)
-        tot += npk
-        e[2].record()
-        d2h = 0
-        for grp, n in names:
-            src = getattr(W, grp)[n]
-            cnt = out_count(grp, n, npk)
-            if out_host[n].numel() < cnt:     # more peaks than the warm-up step found
-                out_host[n] = torch.empty(cnt, dtype=src.dtype).pin_memory()
-            out_host[n][:cnt].copy_(src[:cnt], non_blocking=True)
-            d2h += cnt * src.element_size()
-        out_host["mask"].copy_(W.mask, non_blocking=True)
-        d2h += W.mask.numel() * W.mask.element_size()
-        nh = W.halos.numel()
-        if out_host["halos"].numel() < nh:
-            out_host["halos"] = torch.empty(nh, dtype=torch.float32).pin_memory()
-        out_host["halos"][:nh].copy_(W.halos.reshape(-1), non_blocking=True)
-        d2h += nh * 4
-        e[3].record()
-        torch.cuda.synchronize()
-        parts["h2d_delta"] += e[0].elapsed_time(e[1])
-        parts["step"] += e[1].elapsed_time(e[2])
-        parts["d2h"] += e[2].elapsed_time(e[3])
+            f = torch.cuda.Event()
+            f.record(up)
+        return d, f
+
+    def fetch(dst, src):
+        """Device -> pinned host copy on the download stream (src kept alive for it)."""
+        if dst.numel() < src.numel():
+            dst = torch.empty(src.numel(), dtype=src.dtype).pin_memory()
+        with torch.cuda.stream(down):
+            dst.reshape(-1)[:src.numel()].copy_(src.reshape(-1), non_blocking=True)
+        src.record_stream(down)
+        st["d2h"] += src.numel() * src.element_size()
+        return dst
+
+    def after(stream_wait):
+        e = torch.cuda.Event()
+        e.record(main)
+        stream_wait.wait_event(e)
+
+    ref_npk = W.npeaks                                  # the device-resident steps' count
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s0, s1 = mk(), mk()
+    s0.record()
+    up.wait_stream(main)
+    ready = upload()
+    for s in range(K):
+        cur = {"ready": ready}
+        st["d2h"] = 0
+
+        def on_start(cur=cur):
+            main.wait_event(cur["ready"][0])            # this step's delta is up
+            if st["peaks_done"] is not None:            # the previous peaks are down
+                main.wait_event(st["peaks_done"])
+
+        def on_graph(npk):
+            after(down)
+            for grp, n in names[:5]:
+                out_host[n] = fetch(out_host[n], W.peaks[n][:npk])
+            e = torch.cuda.Event()
+            e.record(down)
+            st["peaks_done"] = e
+
+        def next_inputs(s=s):
+            if s + 1 < K:                               # the tile is free: next inputs up
+                after(up)
+                st["next"] = upload()
+
+        def on_pack():
+            if W.mode != "plain":                       # the walk reads the cell records
+                next_inputs()
+
+        def on_walk():
+            if st["res_done"] is not None:              # the previous results are down
+                main.wait_event(st["res_done"])
+
+        def on_end(npk):
+            if W.mode == "plain":                       # the walk read the fields in place
+                next_inputs()
+            mask_out.copy_(W.mask)                      # after the previous read-back (walk)
+            after(down)
+            for grp, n in names[5:]:
+                out_host[n] = fetch(out_host[n], W.results[n][:out_count(grp, n, npk)])
+            out_host["mask"] = fetch(out_host["mask"], mask_out)
+            out_host["halos"] = fetch(out_host["halos"], W.halos)
+            e = torch.cuda.Event()
+            e.record(down)
+            st["res_done"] = e
+
+        npk = W.step(fields_ready=ready[1],
+                     hooks={"start": on_start, "graph": on_graph, "pack": on_pack,
+                            "walk": on_walk, "end": on_end})
+        st["tot"] += npk
+        ready = st.pop("next", None)
+    main.wait_stream(down)
+    main.wait_stream(up)
     s1.record()
     torch.cuda.synchronize()
+    if st["tot"] != K * ref_npk:        # the same tile every step: the same peaks
+        raise RuntimeError(f"end-to-end steps found {st['tot']} peaks, expected {K} x {ref_npk}")
     ms = s0.elapsed_time(s1)
-    k = max(1, args.e2e_steps)
-    return {"value": tot / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "ms_per_step": ms / k,
-            "parts_ms": {p: v / k for p, v in parts.items()},
+    return {"value": st["tot"] / (ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(st["d2h"]), "ms_per_step": ms / K, "steps": K,
+            "pipelined": "uploads of step s+1 and read-backs of step s overlap compute",
             "wall_s": time.perf_counter() - t0}
 
 
@@ -738,7 +802,7 @@ def main():
     ap.add_argument("--autotune", type=int, default=1,
                     help="time the result-neutral launch parameters once and keep the best")
     ap.add_argument("--seed", type=int, default=12345)
-    ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=4)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=20.0)
     args = ap.parse_args()
