@@ -49,10 +49,21 @@ __device__ int hunt(const double* xx, int n, double x) {
     return jlo;
 }
 
+// The same index from a starting guess: jlo is the number of entries below x (0 when x
+// is NaN), which any search returns; the integration's a only grows, so a walk from the
+// previous call's index takes a step or none instead of eleven dependent loads.
+__device__ int hunt_from(const double* xx, int n, double x, int j) {
+    while (j < n && x > xx[j]) ++j;
+    while (j > 0 && !(x > xx[j - 1])) --j;
+    return j;
+}
+
 // Interpolation window and Lagrange weights of Dlinear_ab / Dfnofa (Cosmology.jl:80-115,
-// 287-330); a 4-point window never starts before the first entry.
-__device__ int growth_weights(const GrowthDev& g, double x, int* k0, double* w) {
-    const int kk = hunt(g.atab, g.ntab, x);
+// 287-330); a 4-point window never starts before the first entry.  *hint (nullable) holds
+// the previous call's table index.
+__device__ int growth_weights(const GrowthDev& g, double x, int* k0, double* w,
+                              int* hint = nullptr) {
+    const int kk = hint ? (*hint = hunt_from(g.atab, g.ntab, x, *hint)) : hunt(g.atab, g.ntab, x);
     int nl;
     if (kk < 2 || kk >= g.ntab) {
         nl = 2;
@@ -80,11 +91,12 @@ __device__ double lagr(const double* v, int nl, const double* w) {
 }
 
 // Dlinear_ab (Cosmology.jl:287-307): D(a) and dlnD/dlna.
-__device__ void dlinear_ab(const GrowthDev& g, double ai, double* dlin, double* hd) {
+__device__ void dlinear_ab(const GrowthDev& g, double ai, double* dlin, double* hd,
+                           int* hint = nullptr) {
     if (ai > g.amin && ai < g.amax) {
         int k0;
         double w[4];
-        const int nl = growth_weights(g, ai, &k0, w);
+        const int nl = growth_weights(g, ai, &k0, w, hint);
         *dlin = lagr(g.Da + k0, nl, w) * ai;
         *hd = lagr(g.f + k0, nl, w);
     } else if (ai >= g.amax) {
@@ -108,33 +120,61 @@ __device__ double dfnofa(const GrowthDev& g, double ai) {
     return ai * g.D_inf;
 }
 
-// Carlson's RD (EllipsoidalCollapse.jl:62-106).  Finite positive arguments converge in a
-// few dozen duplication rounds; the loop stops after kRdMaxIt at the latest (the reference
+// Carlson's RD (EllipsoidalCollapse.jl:62-106), two argument sets side by side: each set
+// runs its own duplication rounds until its own stopping test holds (a finished set stops
+// changing) and then the final formula, so both results are those of two separate calls,
+// while the two square-root / division chains overlap.  Finite positive arguments converge
+// in a few dozen rounds; a set stops after kRdMaxIt rounds at the latest (the reference
 // loops for ever on NaN arguments), as the CPU restatement does.
-__device__ double elliptic_rd(double x, double y, double z) {
-    const double ERRTOL = 0.05, C1 = 3.0 / 14.0, C2 = 1.0 / 6.0, C3 = 9.0 / 22.0,
-                 C4 = 3.0 / 26.0, C5 = 0.25 * C3, C6 = 1.5 * C4;
-    double xt = x, yt = y, zt = z, sum = 0.0, fac = 1.0, delx = 0.0, dely = 0.0, delz = 0.0,
-           ave = 0.0;
-    for (int it = 0; it < kRdMaxIt; ++it) {
-        const double sqrtx = sqrt(xt), sqrty = sqrt(yt), sqrtz = sqrt(zt);
-        const double alamb = sqrtx * (sqrty + sqrtz) + sqrty * sqrtz;
-        sum += fac / (sqrtz * (zt + alamb));
-        fac *= 0.25;
-        xt = 0.25 * (xt + alamb);
-        yt = 0.25 * (yt + alamb);
-        zt = 0.25 * (zt + alamb);
-        ave = 0.2 * (xt + yt + 3.0 * zt);
-        delx = (ave - xt) / ave;
-        dely = (ave - yt) / ave;
-        delz = (ave - zt) / ave;
-        if (fmax(fmax(fabs(delx), fabs(dely)), fabs(delz)) <= ERRTOL) break;
-    }
+struct RdState {
+    double xt, yt, zt, sum, fac, delx, dely, delz, ave;
+    bool done;
+};
+
+__device__ __forceinline__ void rd_init(RdState& r, double x, double y, double z) {
+    r.xt = x; r.yt = y; r.zt = z; r.sum = 0.0; r.fac = 1.0;
+    r.delx = r.dely = r.delz = r.ave = 0.0;
+    r.done = false;
+}
+
+__device__ __forceinline__ void rd_round(RdState& r) {
+    const double ERRTOL = 0.05;
+    const double sqrtx = sqrt(r.xt), sqrty = sqrt(r.yt), sqrtz = sqrt(r.zt);
+    const double alamb = sqrtx * (sqrty + sqrtz) + sqrty * sqrtz;
+    r.sum += r.fac / (sqrtz * (r.zt + alamb));
+    r.fac *= 0.25;
+    r.xt = 0.25 * (r.xt + alamb);
+    r.yt = 0.25 * (r.yt + alamb);
+    r.zt = 0.25 * (r.zt + alamb);
+    r.ave = 0.2 * (r.xt + r.yt + 3.0 * r.zt);
+    r.delx = (r.ave - r.xt) / r.ave;
+    r.dely = (r.ave - r.yt) / r.ave;
+    r.delz = (r.ave - r.zt) / r.ave;
+    r.done = fmax(fmax(fabs(r.delx), fabs(r.dely)), fabs(r.delz)) <= ERRTOL;
+}
+
+__device__ __forceinline__ double rd_final(const RdState& r) {
+    const double C1 = 3.0 / 14.0, C2 = 1.0 / 6.0, C3 = 9.0 / 22.0, C4 = 3.0 / 26.0,
+                 C5 = 0.25 * C3, C6 = 1.5 * C4;
+    const double delx = r.delx, dely = r.dely, delz = r.delz, ave = r.ave;
     const double ea = delx * dely, eb = delz * delz, ec = ea - eb, ed = ea - 6.0 * eb,
                  ee = ed + ec + ec;
-    return 3.0 * sum + fac * (1.0 + ed * (-C1 + C5 * ed - C6 * delz * ee) +
-                              delz * (C2 * ee + delz * (-C3 * ec + delz * C4 * ea))) /
-                           (ave * sqrt(ave));
+    return 3.0 * r.sum + r.fac * (1.0 + ed * (-C1 + C5 * ed - C6 * delz * ee) +
+                                  delz * (C2 * ee + delz * (-C3 * ec + delz * C4 * ea))) /
+                             (ave * sqrt(ave));
+}
+
+__device__ void elliptic_rd2(double x1, double y1, double z1, double x2, double y2, double z2,
+                             double* r1, double* r2) {
+    RdState a, b;
+    rd_init(a, x1, y1, z1);
+    rd_init(b, x2, y2, z2);
+    for (int it = 0; it < kRdMaxIt && !(a.done && b.done); ++it) {
+        if (!a.done) rd_round(a);
+        if (!b.done) rd_round(b);
+    }
+    *r1 = rd_final(a);
+    *r2 = rd_final(b);
 }
 
 // Shape integrals (EllipsoidalCollapse.jl:108-146, iwant_rd = 1).
@@ -163,8 +203,10 @@ __device__ void get_b_2(double a1, double a2, double a3, double* b) {
         return;
     }
     const double r_22 = r_2 * r_2, r_32 = r_3 * r_3, qrat = third * r_2 * r_3;
-    const double b3 = qrat * elliptic_rd(r_22, 1.0, r_32);
-    const double b2 = qrat * elliptic_rd(r_32, 1.0, r_22);
+    double rd3, rd2;
+    elliptic_rd2(r_22, 1.0, r_32, r_32, 1.0, r_22, &rd3, &rd2);
+    const double b3 = qrat * rd3;
+    const double b2 = qrat * rd2;
     b[0] = 1.0 - (b2 + b3);
     b[1] = b2;
     b[2] = b3;
@@ -173,6 +215,7 @@ __device__ void get_b_2(double a1, double a2, double a3, double* b) {
 // DerivState (EllipsoidalCollapse.jl:174-191).
 struct DState {
     int lvirv[3];
+    int hint;             // growth-table index of the last lookup
     double a_3eq, a_2eq, a_1eq, a_3eq2, a_3eq1, Ha;
     double aLam[3], Frho_3;
 };
@@ -224,7 +267,7 @@ __device__ void get_derivs(const EllDev& e, const GrowthDev& g, double t, double
         d1_int = 1.5 * (delta1_e - 1.0) / a_b3 * Ha_inv;
         if (e.fs == 4 || e.fs == 5 || e.fs == 6) {
             double dlin, hd;
-            dlinear_ab(g, a_b, &dlin, &hd);
+            dlinear_ab(g, a_b, &dlin, &hd, &ds.hint);
             d1_ext = 1.5 / a_b3 * Ha_inv * dlin;
         } else if (e.fs == 3) {
             d1_ext = 1.5 * 2.5 / a_b3 * Ha_inv;
@@ -284,6 +327,7 @@ __global__ void __launch_bounds__(kEvolveThreads) evolve_kernel(
     const double Frho = Frho_in[q], e_v = ev_in[q], p_v = pv_in[q];
     DState ds;
     ds.lvirv[0] = ds.lvirv[1] = ds.lvirv[2] = 0;
+    ds.hint = 0;
     ds.a_3eq = ds.a_2eq = ds.a_1eq = ds.a_3eq2 = ds.a_3eq1 = 0.0;
     ds.aLam[2] = Frho / 3.0 * (1.0 + 3.0 * e_v + p_v);
     ds.aLam[1] = Frho / 3.0 * (1.0 - 2.0 * p_v);
