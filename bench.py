@@ -460,8 +460,44 @@ def run_ours(args, rank, world, device):
         "clocks": ck,
         "e2e": e2e,
     }
+    line["post_step_ms"] = post_step(ht, W)
     line["cpu_baseline"] = cpu_baseline(ht, W, args) if args.cpu_seconds > 0 else None
     return line
+
+
+def post_step(ht, W, reps=3):
+    """The stage after the step, outside the timed region: the Lagrangian exclusion of the
+    step's halo records (Merger.merge_catalog, ht_merge_halos) without and with volume
+    reduction, and the Eulerian positions of the survivors (finalize_eulerian), CUDA events
+    on the current stream, mean of `reps` after one warm-up call."""
+    import torch
+    cat = ht.catalog
+    rec = W.halos.contiguous()
+    out = {"halos_in": int(rec.shape[0])}
+    for name, kw in (("merge_halos", {}), ("merge_halos_volume_reduction",
+                                          {"volume_reduction": True})):
+        kept = cat.merge_halos(W.finder, rec, **kw)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            kept = cat.merge_halos(W.finder, rec, **kw)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = a.elapsed_time(b) / reps
+        out[name + "_kept"] = int(kept.shape[0])
+    kept = cat.merge_halos(W.finder, rec)
+    fin = kept.clone()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        fin.copy_(kept)
+        cat.finalize_eulerian(W.finder, fin, (0.0, 0.0, 0.0), ievol=0, z_out=0.0)
+    b.record()
+    torch.cuda.synchronize()
+    out["finalize_eulerian"] = a.elapsed_time(b) / reps
+    return out
 
 
 def run_e2e(ht, W, args):
