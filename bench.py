@@ -838,7 +838,7 @@ def main():
     ap.add_argument("--autotune", type=int, default=1,
                     help="time the result-neutral launch parameters once and keep the best")
     ap.add_argument("--seed", type=int, default=12345)
-    ap.add_argument("--e2e-steps", type=int, default=4)
+    ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=20.0)
     args = ap.parse_args()

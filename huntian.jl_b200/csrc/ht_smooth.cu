@@ -873,27 +873,20 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
             break;
         }
         float2* col = slots + s * S;
-        // half-length packing in place: lane handles the pair (k, M - k), k <= M / 2
-        for (int k = lane; k <= M / 2; k += 32) {
-            const float2 xa = col[k], xb = col[M - k];
-            auto pack = [&](float2 a, float2 bb, int kk) {
-                const float2 b = make_float2(bb.x, -bb.y);      // conj X[M - kk]
-                const float2 e = make_float2(a.x + b.x, a.y + b.y);
-                const float2 d = make_float2(a.x - b.x, a.y - b.y);
-                const float2 wv = __ldg(twp + kk);              // e^{2 pi i kk / N}
-                const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
-                return make_float2(e.x - o.y, e.y + o.x);
-            };
-            const float2 zk = pack(xa, xb, k);
-            const int kh = M - k;
-            if (kh != k && kh < M) col[kh] = pack(xb, xa, kh);
-            col[k] = zk;
-        }
-        __syncwarp();
+        // half-length packing on the way into registers: lane's point k = lane + 32 t is
+        // z_k = (X[k] + conj X[M-k]) + i e^{2 pi i k/N} (X[k] - conj X[M-k]), from the raw
+        // row (no packed copy is written back to shared memory)
         htfft::C2 v[TH];
 #pragma unroll
         for (int t = 0; t < TH; ++t) {
-            v[t] = htfft::to_c2(col[lane + 32 * t]);
+            const int k = lane + 32 * t;
+            const float2 a = col[k], bb = col[M - k];
+            const float2 b = make_float2(bb.x, -bb.y);          // conj X[M - k]
+            const float2 e = make_float2(a.x + b.x, a.y + b.y);
+            const float2 d = make_float2(a.x - b.x, a.y - b.y);
+            const float2 wv = __ldg(twp + k);                   // e^{2 pi i k / N}
+            const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
+            v[t] = htfft::to_c2(make_float2(e.x - o.y, e.y + o.x));
         }
         htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
         __syncwarp();
