@@ -56,6 +56,10 @@ WORKLOADS = {
     "box128": dict(n=128, L=250.0, nbuff=36, nf=30, rmin=2.0, rmax=40.0,
                    desc="128^3 periodic box + 36-cell wrap = 200^3 tile, L=250 Mpc/h, "
                         "30 top-hat filters R=2-40 Mpc/h"),
+    # the large tile's geometry at a size an ncu capture of the walk can replay
+    "tile320": dict(n=192, L=281.25, nbuff=64, nf=80, rmin=1.5, rmax=80.0,
+                    desc="192^3 core + 64-cell buffer = 320^3 tile at the 1152 tile's cell "
+                         "size (L=281.25 Mpc/h, nhunt 63), 80 top-hat filters R=1.5-80 Mpc/h"),
 }
 METRIC = "peaks/s thru peakfind+shell collapse"
 UNIT = "peaks/s"
@@ -326,32 +330,72 @@ class Workload:
         call("end", npk)
         return npk
 
-    def time_walk(self, reps=2):
-        """Walk-only timing on the current peaks (the autotuner's probe)."""
+    def _walk_args(self):
         npk = self.npeaks
         fidx = self.peaks["filter_idx"][:npk].long() - 1
-        args = (self.peaks["i"][:npk], self.peaks["j"][:npk], self.peaks["k"][:npk],
+        return (self.peaks["i"][:npk], self.peaks["j"][:npk], self.peaks["k"][:npk],
                 self.Rf_f[fidx], self.ir2_f[fidx],
                 torch.full((npk,), self.ZZon, dtype=torch.float32, device=self.device),
                 torch.full((npk,), self.fcrit, dtype=torch.float32, device=self.device))
-        cost = None
-        if self.mode == "learned":
-            br = self.ht.bracket
-            F = br.features(self.finder, *args, self.alatt,
-                            peak_delta=self.peaks["delta"][:npk])
-            cost = br.predict(self.finder, self.model, F)[:, 1].contiguous()
+
+    def _cost(self, args):
+        br = self.ht.bracket
+        model = getattr(self, "model", None) or br.BracketModel.load(device=self.device)
+        self.model = model
+        F = br.features(self.finder, *args, self.alatt, peak_delta=self.peaks["delta"][:self.npeaks])
+        return br.predict(self.finder, model, F)[:, 1].contiguous()
+
+    def time_walk(self, reps=2, mode=None, out=None):
+        """Walk-only timing on the current peaks (the autotuner's probe): the min over
+        reps of CUDA events around the call (learned mode: with the features and the MLP)."""
+        mode = mode or self.mode
+        args = self._walk_args()
         best = None
         for _ in range(reps):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             self.mask.zero_()
             a.record()
+            cost = self._cost(args) if mode == "learned" else None
             self.finder.analyse(*args, self.alatt, nbuff=self.nbuff, mask=self.mask,
-                                mode=self.mode, out=self.results, cost=cost)
+                                mode=mode, out=out if out is not None else self.results,
+                                cost=cost)
             b.record()
             torch.cuda.synchronize()
             t = a.elapsed_time(b)
             best = t if best is None else min(best, t)
         return best
+
+    def walk_modes(self, reps=2):
+        """The metric's comparison on this step's peaks: the walk (shell collapse of every
+        peak, CUDA events) in the PLAIN mode (the reference's layout: fields read in place,
+        peaks in batch order, static schedule), BATCHED (packed cell records, spatial
+        order, persistent queue) and LEARNED (BATCHED ordered by the learned bracket, the
+        features and the MLP inside the timed call), with a checksum of every result
+        array and of the mask per mode: the three must be identical."""
+        res = self.ht.HaloFinder.alloc_results(self.npeaks, self.device)
+        out = {"walk_ms": {}, "checksum": {}}
+        for mode in ("plain", "batched", "learned"):
+            out["walk_ms"][mode] = self.time_walk(reps, mode, res)
+            h = 0
+            for k in self.ht.RESULT_NAMES:
+                v = res[k][: self.npeaks * self.ht.RESULT_WIDTH.get(k, 1)].view(torch.int32)
+                h = (h * 1000003 + int(v.long().sum().item())) % (1 << 61)
+            h = (h * 1000003 + int(self.mask.long().sum().item())) % (1 << 61)
+            out["checksum"][mode] = h
+        ck = out["checksum"]
+        out["identical"] = ck["plain"] == ck["batched"] == ck["learned"]
+        w = out["walk_ms"]
+        out["speedup_learned_vs_plain"] = w["plain"] / w["learned"]
+        out["speedup_learned_vs_batched"] = w["batched"] / w["learned"]
+        return out
+
+    def release_smoothing(self):
+        """Drop the CUDA graph and the smoothing buffers (after the timed steps)."""
+        self.graph = None
+        self.pk = None
+        self.dk = None
+        self._ds = None
+        torch.cuda.empty_cache()
 
     def autotune(self):
         """Pick the result-neutral launch parameters by timing them on this workload: the
@@ -461,7 +505,10 @@ def run_ours(args, rank, world, device):
         "e2e": e2e,
     }
     line["post_step_ms"] = post_step(ht, W)
-    line["cpu_baseline"] = cpu_baseline(ht, W, args) if args.cpu_seconds > 0 else None
+    line["walk_modes"] = W.walk_modes() if args.compare_modes else None
+    W.release_smoothing()
+    if args.cpu_seconds > 0:
+        line["cpu_baseline"], line["parity"] = cpu_baseline(ht, W, args)
     return line
 
 
@@ -628,96 +675,289 @@ def run_e2e(ht, W, args):
             "wall_s": time.perf_counter() - t0}
 
 
-def cpu_baseline(ht, W, args, steps=1):
-    """Time the CPU oracle on host cores on a bounded sample of this workload:
-    (a) RadialShell.analyse_peak on a random sample of the step's peaks, all threads;
-    (b) PeakFind.find_peaks on a 128^3 sub-block of every filter's smoothed field.
-    Per-peak CPU time = shell time per peak + (scan time per cell x tile cells x filters)
-    / peaks."""
+# ------------------------------------------------------------- CPU legs ----
+#
+# The reference's CPU path -- PeakFind.find_peaks over every filter with the mask carried,
+# then RadialShell.analyse_peak per peak (src/HaloFinder/PeakFind.jl:15-78,
+# src/HaloFinder/RadialShell.jl:281-865) -- timed on the host cores through the oracle (its
+# C restatement, OpenMP over peaks as Pipeline.jl:235-242 threads them).  These legs call
+# no function of the CUDA library: the fields come from synth (torch) and the smoothing
+# from torch.fft with the top-hat window of Filters.smooth_field.  The walk of one peak
+# of the large tile costs the CPU path about 0.1 s (every one of its 3,310 shells), so a
+# step times a bounded sample: every filter's peaks in a central sub-volume (found by the
+# oracle), a random sample of them analysed, and the find cost per cell of 130^3 blocks;
+# the rate is per peak of that sample, extrapolated in no other way.
+
+SUB = 64          # side of the central sub-volume whose peaks the CPU legs analyse
+PARITY_PEAKS = 300
+
+
+def torch_smooth(dk, n, boxsize, Rf):
+    """Top-hat smoothed tile from its rfft (torch/cuFFT, not the library): the window
+    3 (sin x - x cos x) / x^3 of Filters.smooth_field (ext/CUDAExt.jl:2853-2866) per integer
+    |k|^2 in FP64, rounded to Float32, times the spectrum, inverse rfft."""
+    import torch
+    dev = dk.device
+    q = np.arange(3 * (n // 2) ** 2 + 1, dtype=np.float64)
+    x = np.sqrt(q) * (2 * math.pi / boxsize) * Rf
+    with np.errstate(invalid="ignore", divide="ignore"):
+        w = 3.0 * (np.sin(x) - x * np.cos(x)) / x ** 3
+    w[0] = 1.0
+    tab = torch.tensor(w.astype(np.float32), device=dev)
+    iz = torch.arange(n, device=dev)
+    sz = torch.where(iz <= n // 2, iz, iz - n)
+    ix = torch.arange(n // 2 + 1, device=dev)
+    out = torch.empty_like(dk)
+    for z0 in range(0, n, 64):
+        z1 = min(n, z0 + 64)
+        qq = sz[z0:z1, None, None] ** 2 + sz[None, :, None] ** 2 + ix[None, None, :] ** 2
+        out[z0:z1] = dk[z0:z1] * tab[qq]
+    return torch.fft.irfftn(out, s=(n, n, n), dim=(0, 1, 2))
+
+
+class CpuLeg:
+    """The CPU path on a bounded sample of a tile workload (see the section comment)."""
+
+    def __init__(self, tile, filters, alatt, nbuff, nhunt, fcrit, ZZon, table_path):
+        import torch
+        import oracle
+        oracle.build()
+        self.oracle = oracle
+        self.nthreads = oracle.max_threads()
+        self.filters, self.alatt, self.nbuff, self.nhunt = filters, alatt, nbuff, nhunt
+        self.fcrit, self.ZZon = fcrit, ZZon
+        self.ct = oracle.read_homeltab(table_path)
+        self.shells = oracle.precompute_shells(nhunt)
+        nt = tile["delta"].shape[0]
+        self.nt = nt
+        dk = torch.fft.rfftn(tile["delta"], dim=(0, 1, 2))
+        # central sub-volume [s0, s0 + SUB) (0-based) on the tile's diagonal, so that the
+        # transposed reads delta[k, i, j] of its walks stay inside the sub-tile below
+        self.s0 = s0 = nt // 2 - SUB // 2
+        self.o = o = s0 - nhunt - 1             # sub-tile origin (0-based)
+        m = SUB + 2 * (nhunt + 1)
+        self.sub = {k: np.ascontiguousarray(v[o:o + m, o:o + m, o:o + m].cpu().numpy())
+                    for k, v in tile.items()}
+        self.F = oracle.Fields(self.sub["delta"], self.sub["etax"], self.sub["etay"],
+                               self.sub["etaz"], self.sub.get("eta2x"), self.sub.get("eta2y"),
+                               self.sub.get("eta2z"))
+        # every filter's peaks in the sub-volume (mask carried), and 130^3 blocks of some
+        # filters' smoothed fields for the find timing
+        mask = np.zeros((SUB + 2,) * 3, np.int8)
+        pi, pj, pk, pf = [], [], [], []
+        self.blocks = []
+        c0, bsz = nbuff, 130
+        step = max(1, len(filters) // 8)
+        for fi, flt in enumerate(filters):
+            ds = torch_smooth(dk, nt, nt * alatt, flt[2])
+            blk = ds[s0 - 1:s0 + SUB + 1, s0 - 1:s0 + SUB + 1, s0 - 1:s0 + SUB + 1].cpu().numpy()
+            i, j, k, _ = oracle.find_peaks(blk, mask, 1, fcrit)
+            pi.append(i + s0 - 1); pj.append(j + s0 - 1); pk.append(k + s0 - 1)
+            pf.append(np.full(len(i), fi))
+            if fi % step == 0:
+                self.blocks.append(np.ascontiguousarray(
+                    ds[c0:c0 + bsz, c0:c0 + bsz, c0:c0 + bsz].cpu().numpy()))
+            del ds
+        del dk
+        self.pi, self.pj, self.pk = (np.concatenate(v) for v in (pi, pj, pk))
+        self.pf = np.concatenate(pf)
+        self.Rf_all = np.array([f[2] for f in filters])
+        self.ir2_all = np.array([min(math.floor((1.75 * f[2] / alatt) ** 2),
+                                     math.floor((40.0 / alatt - 1) ** 2)) for f in filters])
+        self.rng = np.random.default_rng(0)
+
+    def analyse(self, pi, pj, pk, fidx, kind="radialshell", exact=False):
+        """Oracle results for tile peaks (1-based tile coordinates) on the sub-tile."""
+        o = self.o
+        return self.oracle.analyse_batch(
+            self.F, pi - o, pj - o, pk - o, self.ir2_all[fidx], self.Rf_all[fidx], self.ZZon,
+            np.float32(self.fcrit), self.alatt, self.ct, self.shells, kind=kind,
+            nthreads=self.nthreads, exact_products=exact)[0]
+
+    def sample(self, budget):
+        """One timed sample: find_peaks on the 130^3 blocks (one thread, as the
+        reference's scan), analyse_peak on random sub-volume peaks (all threads)."""
+        t_find, cells = 0.0, 0
+        for blk in self.blocks:
+            mask = np.zeros(blk.shape, np.int8)
+            t0 = time.perf_counter()
+            self.oracle.find_peaks(blk, mask, 1, self.fcrit)
+            t_find += time.perf_counter() - t0
+            cells += (blk.shape[0] - 2) ** 3
+        per_cell = t_find / cells
+        npk = len(self.pi)
+        t_sh, done, batch = 0.0, 0, max(2 * self.nthreads, 32)
+        while t_sh < budget and done < npk:
+            idx = self.rng.choice(npk, size=min(batch, npk), replace=False)
+            t0 = time.perf_counter()
+            self.analyse(self.pi[idx], self.pj[idx], self.pk[idx], self.pf[idx])
+            t_sh += time.perf_counter() - t0
+            done += len(idx)
+            batch = min(2 * batch, 2048)
+        per_peak_shell = t_sh / max(done, 1)
+        # find cost per peak: every filter scans every cell once; the sub-volume tells the
+        # cells per peak of this workload
+        per_peak_find = per_cell * len(self.filters) * SUB ** 3 / max(npk, 1)
+        return {"value": 1.0 / (per_peak_shell + per_peak_find), "unit": UNIT,
+                "cores": self.nthreads, "kind": "port",
+                "sample": f"C restatement of RadialShell.analyse_peak (FP64, {self.nthreads} "
+                          f"threads) on {done} random peaks of the {npk} that find_peaks finds "
+                          f"in the central {SUB}^3 sub-volume (all {len(self.filters)} "
+                          f"filters, mask carried); find_peaks (1 thread) timed on 130^3 "
+                          f"blocks of {len(self.blocks)} filters' fields; per-peak costs of "
+                          f"this sample",
+                "shell_s_per_peak": per_peak_shell, "find_s_per_cell": per_cell,
+                "find_s_per_peak": per_peak_find}
+
+    def parity(self, ht, finder, peaks, results, npk_all):
+        """Device results of the timed step for step peaks inside the sub-volume (GPU
+        convention, as the step ran) and the library's CPU convention on the same peaks,
+        against both oracle variants (oracle/parity.py)."""
+        import torch
+        from oracle import parity
+        s0 = self.s0
+        pi, pj, pk = (peaks[c][:npk_all].cpu().numpy() for c in ("i", "j", "k"))
+        inside = np.flatnonzero((pi - 1 >= s0) & (pi - 1 < s0 + SUB) & (pj - 1 >= s0) &
+                                (pj - 1 < s0 + SUB) & (pk - 1 >= s0) & (pk - 1 < s0 + SUB))
+        sel = np.sort(self.rng.choice(inside, size=min(PARITY_PEAKS, len(inside)),
+                                      replace=False))
+        fidx = peaks["filter_idx"][:npk_all].cpu().numpy()[sel] - 1
+        width = ht.RESULT_WIDTH
+        rows = lambda res, n, idx: {k: res[k][:n * width.get(k, 1)].cpu().numpy()
+                                    .reshape(n, -1)[idx] for k in ("RTHL", "Fbarx", "e_v",
+                                    "p_v", "Srb", "d2F", "zvir_half", "Sbar", "Sbar2", "gradpk",
+                                    "gradpkf", "gradpkrf", "strain", "eigs")}
+        out = {"peaks_in_subvolume": int(len(inside))}
+        t0 = time.perf_counter()
+        g_gpu = rows(results, npk_all, sel)
+        ox = self.analyse(pi[sel], pj[sel], pk[sel], fidx, "cudakernel", exact=True)
+        o = self.analyse(pi[sel], pj[sel], pk[sel], fidx, "cudakernel")
+        out["gpu_convention"] = parity.report(g_gpu, o, ora_exact=ox, max_list=5)
+        out["gpu_convention_vs_full_fp64"] = parity.report(g_gpu, ox, max_list=5)
+        # the same peaks through the library's CPU convention (RadialShell.analyse_peak)
+        dev = peaks["i"].device
+        ti = lambda a: torch.as_tensor(a, dtype=torch.int32, device=dev)
+        n = len(sel)
+        res = finder.analyse(ti(pi[sel]), ti(pj[sel]), ti(pk[sel]),
+                             torch.as_tensor(self.Rf_all[fidx], dtype=torch.float64, device=dev),
+                             ti(self.ir2_all[fidx]),
+                             torch.full((n,), self.ZZon, dtype=torch.float32, device=dev),
+                             torch.full((n,), self.fcrit, dtype=torch.float32, device=dev),
+                             self.alatt, conv="cpu", mode="plain")
+        torch.cuda.synchronize()
+        g_cpu = rows(res, n, np.arange(n))
+        ox = self.analyse(pi[sel], pj[sel], pk[sel], fidx, "radialshell", exact=True)
+        o = self.analyse(pi[sel], pj[sel], pk[sel], fidx, "radialshell")
+        out["cpu_convention"] = parity.report(g_cpu, o, ora_exact=ox, max_list=5)
+        out["oracle_s"] = time.perf_counter() - t0
+        return out
+
+
+def full_config1_cpu():
+    """The reference's CPU path on the whole small box (128^3, L = 250 Mpc/h, 36-cell
+    wrap, 30 top-hat filters R = 2-40 Mpc/h, seed 12345), unsampled: find_peaks over every
+    filter (one thread, mask carried) and analyse_peak on every peak (all threads)."""
     import torch
     import oracle
-    oracle.build()
-    nthreads = oracle.max_threads()
-    npk = W.npeaks
-    rng = np.random.default_rng(0)
-    budget = args.cpu_seconds
-    # --- shell collapse sample
-    sl = {k: v.cpu().numpy() for k, v in W.tile.items()}
-    F = oracle.Fields(sl["delta"], sl["etax"], sl["etay"], sl["etaz"], sl["eta2x"], sl["eta2y"],
-                      sl["eta2z"])
-    tab, axes = ht.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
-    ct = oracle.CollapseTable(tab, *axes)
-    shells = oracle.precompute_shells(W.nhunt)
-    pi = W.peaks["i"][:npk].cpu().numpy(); pj = W.peaks["j"][:npk].cpu().numpy()
-    pk = W.peaks["k"][:npk].cpu().numpy(); fi = W.peaks["filter_idx"][:npk].cpu().numpy() - 1
-    Rf_all = np.array([f[2] for f in W.filters]); ir2_all = W.ir2_f.cpu().numpy()
-    sample, t_shell = 0, 0.0
-    batch = max(4 * nthreads, 64)
-    order = rng.permutation(npk)
-    pos = 0
-    while t_shell < budget * 0.6 and pos < npk:
-        idx = order[pos:pos + batch]
-        pos += len(idx)
+    _package()
+    from huntian_b200 import synth, tables
+    n, L, nbuff, nf = 128, 250.0, 36, 30
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cosmo = synth.Cosmology()
+    dk0 = synth.gaussian_box(n, L, 12345, cosmo, dev)
+    psi1, psi2 = synth.displacements(dk0, n, L, ilpt=2)
+    tile = {"delta": synth.wrap_pad(synth._irfft(dk0, n), nbuff)}
+    for nm, t in zip(("etax", "etay", "etaz", "eta2x", "eta2y", "eta2z"), psi1 + psi2):
+        tile[nm] = synth.wrap_pad(t, nbuff)
+    nt, alatt = n + 2 * nbuff, L / n
+    filters = tables.log_filterbank(nf, 2.0, 40.0)
+    ct = oracle.read_homeltab(os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+    fcrit = float(np.float32(ct.fsc_of_z(0.0)))
+    nhunt = min(nbuff - 1, math.floor(filters[0][2] * 1.75 / alatt))
+    dk = torch.fft.rfftn(tile["delta"], dim=(0, 1, 2))
+    host = {k: v.cpu().numpy() for k, v in tile.items()}
+    mask = np.zeros((nt,) * 3, np.int8)
+    t_find, found = 0.0, []
+    for fi, flt in enumerate(filters):
+        ds = torch_smooth(dk, nt, nt * alatt, flt[2]).cpu().numpy()
         t0 = time.perf_counter()
-        oracle.analyse_batch(F, pi[idx], pj[idx], pk[idx], ir2_all[fi[idx]], Rf_all[fi[idx]],
-                             W.ZZon, -1.0, W.alatt, ct, shells, nbuff=W.nbuff,
-                             kind="radialshell", nthreads=nthreads)
-        t_shell += time.perf_counter() - t0
-        sample += len(idx)
-        batch = min(batch * 2, 4096)
-    per_peak_shell = t_shell / max(sample, 1)
-    # --- peak scan sample: a 130^3 sub-block (128^3 scanned) of each smoothed field
-    b = 130
-    t_find, nfilt = 0.0, 0
-    mask = np.zeros((b, b, b), np.int8)
-    c0 = W.nbuff
-    saved_dk = W.dk          # the CUDA graph (if any) reads this buffer: keep it alive
-    W.dk = torch.fft.rfftn(W.tile["delta"], dim=(0, 1, 2)).contiguous()
-    for flt in W.filters[:: max(1, len(W.filters) // 8)]:
-        ds = W.smooth(flt[2])[c0:c0 + b, c0:c0 + b, c0:c0 + b].cpu().numpy()
-        t0 = time.perf_counter()
-        oracle.find_peaks(ds, mask, 1, W.fcrit)
+        i, j, k, _ = oracle.find_peaks(ds, mask, nbuff, fcrit)
         t_find += time.perf_counter() - t0
-        nfilt += 1
-        if t_find > budget * 0.3:
-            break
-    W.dk = saved_dk
-    per_cell = t_find / (nfilt * 128 ** 3)
-    core = W.nt - 2 * W.nbuff
-    find_tile = per_cell * core ** 3 * len(W.filters)
-    cpu_time = per_peak_shell * npk + find_tile
-    return {"value": npk / cpu_time, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": f"analyse_peak (RadialShell.jl restatement, FP64, {nthreads} threads) on "
-                      f"{sample} random peaks of {npk}; find_peaks on a 128^3 sub-block of "
-                      f"{nfilt} of {len(W.filters)} filters (1 thread), scaled to the tile",
-            "shell_s_per_peak": per_peak_shell, "find_s_per_cell": per_cell}
+        found.append((i, j, k, np.full(len(i), fi)))
+    pi, pj, pk, pf = (np.concatenate([f[c] for f in found]) for c in range(4))
+    Rf = np.array([f[2] for f in filters])[pf]
+    ir2 = np.array([min(math.floor((1.75 * f[2] / alatt) ** 2),
+                        math.floor((40.0 / alatt - 1) ** 2)) for f in filters])[pf]
+    F = oracle.Fields(host["delta"], host["etax"], host["etay"], host["etaz"], host["eta2x"],
+                      host["eta2y"], host["eta2z"])
+    nth = oracle.max_threads()
+    t0 = time.perf_counter()
+    o, _ = oracle.analyse_batch(F, pi, pj, pk, ir2, Rf, 1.0, np.float32(fcrit), alatt, ct,
+                                oracle.precompute_shells(nhunt), nbuff=nbuff,
+                                kind="radialshell", nthreads=nth)
+    t_shell = time.perf_counter() - t0
+    return {"value": len(pi) / (t_find + t_shell), "unit": UNIT, "cores": nth, "kind": "port",
+            "sample": f"unsampled: the whole 128^3 box (200^3 tile, 30 filters): find_peaks "
+                      f"over every filter ({t_find:.2f} s, 1 thread) and RadialShell."
+                      f"analyse_peak on all {len(pi)} peaks ({t_shell:.1f} s, {nth} threads)",
+            "peaks": int(len(pi)), "collapsed": int((o["RTHL"] > 0).sum()),
+            "find_s": t_find, "shell_s": t_shell}
+
+
+def cpu_baseline(ht, W, args):
+    """Our arm's CPU leg (rank 0, N = 1, outside the timed region): the CPU path's rate on
+    a bounded sample of this workload, and the parity of the timed step's results."""
+    leg = CpuLeg(W.tile, W.filters, W.alatt, W.nbuff, W.nhunt, W.fcrit, W.ZZon,
+                 os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat"))
+    cb = leg.sample(args.cpu_seconds)
+    par = leg.parity(ht, W.finder, W.peaks, W.results, W.npeaks)
+    return cb, par
 
 
 def run_reference(args, rank, world, device):
-    """--impl reference: the CPU oracle on the host cores, on bounded samples."""
+    """--impl reference: the reference's CPU path (the oracle) on the host cores, on
+    bounded samples of the same workload; the CUDA library is never loaded."""
     if rank != 0:
         return None
     import torch
-    ht = _package()
-    W = Workload(ht, args.workload, args.seed, device, "batched")
-    W.step()
-    torch.cuda.synchronize()
-    vals = []
-    for s in range(args.warmup + args.steps):
-        cb = cpu_baseline(ht, W, argparse.Namespace(cpu_seconds=args.ref_seconds))
-        if s >= args.warmup:
-            vals.append(cb)
+    _package()          # registers the package (synth, tables); the library stays unloaded
+    from huntian_b200 import synth, tables
+    wl = WORKLOADS[args.workload]
+    n, L, nbuff = wl["n"], wl["L"], wl["nbuff"]
+    alatt = L / n
+    filters = tables.log_filterbank(wl["nf"], wl["rmin"], wl["rmax"])
+    nhunt = min(nbuff - 1, math.floor(filters[0][2] * 1.75 / alatt))
+    cosmo = synth.Cosmology()
+    dk = synth.gaussian_box(n, L, args.seed, cosmo, device)
+    psi1, psi2 = synth.displacements(dk, n, L, ilpt=2)
+    tile = {"delta": synth.wrap_pad(synth._irfft(dk, n), nbuff)}
+    del dk
+    for nm, t in zip(("etax", "etay", "etaz", "eta2x", "eta2y", "eta2z"), psi1 + psi2):
+        tile[nm] = synth.wrap_pad(t, nbuff)
+    del psi1, psi2
+    torch.cuda.empty_cache()
+    import oracle
+    tpath = os.path.join(ROOT, "tests", "golden", "HomelTab_julia.dat")
+    fcrit = float(np.float32(oracle.read_homeltab(tpath).fsc_of_z(0.0)))
+    leg = CpuLeg(tile, filters, alatt, nbuff, nhunt, fcrit, 1.0, tpath)
+    del tile
+    vals = [leg.sample(args.ref_seconds) for _ in range(args.warmup + args.steps)]
+    vals = vals[args.warmup:]
     v = float(np.mean([c["value"] for c in vals]))
     cb = dict(vals[-1])
     cb["value"] = v
-    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * W.npeaks / v,
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * len(leg.pi) / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded BBKS LambdaCDM Gaussian field, 2LPT)",
-            "config": {"workload": args.workload, "desc": W.wl["desc"],
-                       "peaks_per_step": W.npeaks},
+            "config": {"workload": args.workload, "desc": wl["desc"],
+                       "peaks_per_step": int(len(leg.pi)),
+                       "step": f"the peaks of the central {SUB}^3 sub-volume"},
             "impl": "reference", "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.ref_full:
+        line["cpu_baseline_full"] = full_config1_cpu()
+    return line
 
 
 COLLAPSE_METRIC = "ellipsoids/s thru RK4 collapse-table generation"
@@ -840,7 +1080,13 @@ def main():
     ap.add_argument("--seed", type=int, default=12345)
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--ref-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-seconds", type=float, default=4.0,
+                    help="CPU seconds of analyse_peak per step of --impl reference")
+    ap.add_argument("--ref-full", type=int, default=1,
+                    help="--impl reference also times the whole 128^3 box unsampled")
+    ap.add_argument("--compare-modes", type=int, default=1,
+                    help="after the timed steps, time the walk in the PLAIN, BATCHED and "
+                         "LEARNED modes on the same peaks")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 

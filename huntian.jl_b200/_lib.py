@@ -30,6 +30,8 @@ HT_TUNE_BLOCK_BITS = 1
 HT_TUNE_PF_KZ = 2
 HT_TUNE_WALK_BPSM = 3
 HT_TUNE_FFT_PATH = 4
+HT_TUNE_WAIT_NS = 5
+HT_TUNE_INJECT_TX = 6
 
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",

@@ -1,15 +1,13 @@
 """Build recipe for libhuntian_b200.so (sm_100a), in-tree next to this file.
 
-    python huntian.jl_b200/build.py [--verbose] [--smallcase]
+    python huntian.jl_b200/build.py [--verbose]
 
 Compiles every .cu under csrc/ with nvcc for sm_100a only (no fast-math: the collapse
 criterion needs IEEE divisions, square roots and NaN propagation) and links them into
 one shared library with a plain C ABI (include/huntian_b200.h).  The files listed in
 FILE_FLAGS are compiled to objects of their own with extra flags first (ht_collapse.cu
 with -fmad=false: the ellipsoid integration keeps every product unfused, as the
-reference's Julia arithmetic does).  --smallcase also builds
-pencil_smallcase, the reduced-size driver of the 1152^3 pencil smoothing kernels used for
-ncu captures.
+reference's Julia arithmetic does).
 """
 import glob
 import os
@@ -74,21 +72,6 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
-def build_smallcase() -> str:
-    """pencil_smallcase: pencil_smallcase.cu (which includes csrc/ht_smooth.cu) linked with
-    the other sources."""
-    out = os.path.join(HERE, "pencil_smallcase")
-    plain, special = _split_sources([f for f in sources()
-                                     if os.path.basename(f) != "ht_smooth.cu"])
-    objs = _objects(special, FLAGS)
-    srcs = [os.path.join(HERE, "pencil_smallcase.cu")] + plain
-    flags = [f for f in FLAGS if f not in ("-shared", "-Xcompiler", "-fPIC", "-fvisibility=hidden")]
-    subprocess.run([NVCC] + flags + ["-lcuda"] + srcs + objs + ["-o", out], check=True)
-    return out
-
-
 if __name__ == "__main__":
     build(force=True, verbose="--verbose" in sys.argv)
     print(LIB)
-    if "--smallcase" in sys.argv:
-        print(build_smallcase())

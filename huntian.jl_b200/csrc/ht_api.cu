@@ -455,6 +455,16 @@ extern "C" int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value) {
             if (value < 0 || value > 32) return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: blocks per SM must be 0..32");
             ctx->tune_walk_bpsm = (int)value;
             return HT_OK;
+        case HT_TUNE_WAIT_NS:
+            if (value < 1000 || value > 60000000000LL)
+                return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: wait limit must be 1e3..6e10 ns");
+            ctx->wait_ns = (long long)value;
+            return HT_OK;
+        case HT_TUNE_INJECT_TX:
+            if (value < 0 || value > 4096 || value % 16 != 0)
+                return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: injected bytes must be 0..4096, a multiple of 16");
+            ctx->inject_tx = (unsigned)value;
+            return HT_OK;
         default:
             return ht_fail(HT_ERR_INVALID, "ht_ctx_tune: unknown key " + std::to_string(key));
     }

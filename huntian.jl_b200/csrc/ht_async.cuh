@@ -1,17 +1,18 @@
 // Asynchronous-copy helpers shared by the TMA pipelines (peak scan, pencil FFT passes):
 // mbarrier set-up, bounded waits and 1-D bulk copies global -> shared.
 //
-// Every wait is bounded: a wait that has not completed after kWaitNs of %globaltimer
-// returns false, and the kernel records that in the context's status word, drains its own
-// copies in flight (again with bounded waits) and returns, so that a stalled copy shows up
-// as an error code on the host instead of a hung device.
+// Every wait is bounded: a wait that has not completed after its limit of %globaltimer
+// (kWaitNs unless the context sets another, ht_ctx_tune HT_TUNE_WAIT_NS) returns false,
+// and the kernel records that in the context's status word, drains its own copies in
+// flight (again with bounded waits) and returns, so that a stalled copy shows up as an
+// error code on the host instead of a hung device.
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace htasync {
 
-constexpr long long kWaitNs = 2000000000LL;   // 2 s
+constexpr long long kWaitNs = 2000000000LL;   // 2 s, the default limit
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -54,8 +55,9 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
         :: "r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
 }
 
-// Wait for phase `parity` of the barrier, giving up after kWaitNs.
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity) {
+// Wait for phase `parity` of the barrier, giving up after limit_ns.
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parity,
+                                         long long limit_ns = kWaitNs) {
     const unsigned b = smem_addr(bar);
     long long t0 = 0;
     for (int it = 0;; ++it) {
@@ -66,7 +68,7 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parit
                      : "=r"(ok) : "r"(b), "r"(parity) : "memory");
         if (ok) return true;
         if (it == 0) t0 = global_ns();
-        else if ((it & 63) == 0 && global_ns() - t0 > kWaitNs) return false;
+        else if ((it & 63) == 0 && global_ns() - t0 > limit_ns) return false;
     }
 }
 

@@ -46,6 +46,9 @@ struct ht_ctx {
     int tune_walk_bpsm = 0;        // walk: blocks per SM (0: occupancy maximum)
     int tune_fft_path = 0;         // tile smoothing: 0 auto, 1 3-D plan, 2 transposed 1-D,
                                    // 3 fused three-pass, 4 pencil (n = 576, 1152)
+    long long wait_ns = 2000000000LL;  // limit of every bounded in-kernel wait
+    unsigned inject_tx = 0;        // test hook: bytes announced beyond the first copy of
+                                   // every peak-scan CTA (its wait then runs out)
 
     // collapse table + SPH table
     std::vector<float> h_ct;

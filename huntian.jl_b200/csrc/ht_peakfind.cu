@@ -128,11 +128,13 @@ static_assert(kPlaneFloats * kPPS <= kSlotFloats && (kSlotFloats * 4) % 128 == 0
 using htasync::bar_wait;
 using htasync::smem_addr;
 
+// `extra` bytes are announced on top of the copy's own (0 except under the test hook
+// that makes the stage's bounded wait run out: the copy lands, the phase never completes).
 __device__ __forceinline__ void tma_plane(float* dst, const CUtensorMap* tm, int x, int y,
-                                          int z, unsigned long long* bar) {
+                                          int z, unsigned long long* bar, unsigned extra = 0) {
     const unsigned b = smem_addr(bar);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(b), "r"(kPlaneBytes) : "memory");
+                 :: "r"(b), "r"(kPlaneBytes + extra) : "memory");
     asm volatile(
         "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
         "[%0], [%1, {%2, %3, %4}], [%5];"
@@ -146,7 +148,8 @@ __device__ __forceinline__ void tma_plane(float* dst, const CUtensorMap* tm, int
 // across the 3 columns).  A stage is released once both of its planes are folded.
 __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     const __grid_constant__ CUtensorMap tm, const int8_t* __restrict__ mask,
-    PfGeom g, float fcrit, int kz, uint32_t* __restrict__ bits, int32_t* __restrict__ status) {
+    PfGeom g, float fcrit, int kz, uint32_t* __restrict__ bits, int32_t* __restrict__ status,
+    long long wait_ns, unsigned inject_tx) {
     __shared__ __align__(128) float ring[kStages][kSlotFloats];
     __shared__ __align__(8) unsigned long long full[kStages];
     const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kTX + tx;
@@ -179,7 +182,8 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     int issued = 0;   // stages issued (thread 0 only)
     if (tid == 0) {
         for (; issued < kStages && issued < nstages; ++issued)
-            tma_plane(ring[issued], &tm, x0, jb - 1, kb - 1 + kPPS * issued, &full[issued]);
+            tma_plane(ring[issued], &tm, x0, jb - 1, kb - 1 + kPPS * issued, &full[issued],
+                      issued == 0 ? inject_tx : 0u);
     }
     // 3x3 maxima of the thread's 4 cells in plane p, and their centre values
     auto fold = [&](int p, float (&m)[kRowsPT], float (&ctr)[kRowsPT]) {
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     // wait for stage s; false (uniformly) when the wait timed out
     auto wait_stage = [&](int s) {
         s_now = s;
-        const bool ok = bar_wait(&full[s % kStages], (unsigned)((s / kStages) & 1));
+        const bool ok = bar_wait(&full[s % kStages], (unsigned)((s / kStages) & 1), wait_ns);
         return ok;
     };
     // all warps are done with stage s: hand its slot to stage s + kStages
@@ -275,7 +279,7 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
         // record the timeout, then wait (bounded) for the copies still in flight
         atomicExch(status, 1);
         for (int q = s_now; q < issued; ++q)
-            bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1));
+            bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1), wait_ns);
     }
 }
 
@@ -464,7 +468,8 @@ int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_
         if (ctx->tune_pf_kz > 0) kz = ctx->tune_pf_kz;   // autotuned (ht_ctx_tune)
         dim3 grid1(gx, gyb, (unsigned)((g.inner + kz - 1) / kz));
         pf_flag_tma_kernel<<<grid1, dim3(kTX, kTY), 0, st>>>(tm, d_mask, g, fcrit, kz, bits,
-                                                             ht_status_word(ctx));
+                                                             ht_status_word(ctx), ctx->wait_ns,
+                                                             ctx->inject_tx);
         HT_CUDA_TRY(cudaGetLastError(), "pf_flag_tma_kernel launch");
     } else {
         dim3 grid1(gx, gy, (unsigned)((g.inner + kKZ - 1) / kKZ));

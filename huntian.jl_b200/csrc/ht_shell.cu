@@ -282,9 +282,57 @@ __device__ __forceinline__ Strain strain_central(const WalkArgs& a, const double
     return kernel_strain_central(a.rad, a.akk, a.aRnor, P, lo, hi);
 }
 
-// Ascending eigenvalues of a symmetric 3x3 matrix in FP64 by the trigonometric solution
-// of the characteristic cubic (O. K. Smith, Comm. ACM 4(4):168, 1961), replacing LAPACK
-// eigvals(Symmetric) (RadialShell.jl:215-220).  E = (11, 22, 33, 12, 13, 23).
+// Ascending eigenvalues of a symmetric 3x3 matrix by cyclic Jacobi rotations in FP64
+// (Rutishauser's formulation: t = sgn(theta) / (|theta| + sqrt(theta^2 + 1))): backward
+// stable, so every eigenvalue is accurate to a few ulps of the matrix norm even when two
+// of them coincide.  Six sweeps converge a 3x3 matrix to machine precision (quadratic
+// convergence); a rotation whose off-diagonal entry is already zero is skipped.
+__device__ __noinline__ void eig3_jacobi(const double* E, double* lam) {
+    double a00 = E[0], a11 = E[1], a22 = E[2], a01 = E[3], a02 = E[4], a12 = E[5];
+    for (int sweep = 0; sweep < 6; ++sweep) {
+        if (a01 == 0.0 && a02 == 0.0 && a12 == 0.0) break;
+        // (p, q) = (0, 1)
+        if (a01 != 0.0) {
+            const double th = (a11 - a00) / (2.0 * a01);
+            const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+            a00 -= t * a01; a11 += t * a01; a01 = 0.0;
+            const double r0 = a02, r1 = a12;
+            a02 = c * r0 - sn * r1; a12 = sn * r0 + c * r1;
+        }
+        // (p, q) = (0, 2)
+        if (a02 != 0.0) {
+            const double th = (a22 - a00) / (2.0 * a02);
+            const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+            a00 -= t * a02; a22 += t * a02; a02 = 0.0;
+            const double r0 = a01, r1 = a12;
+            a01 = c * r0 - sn * r1; a12 = sn * r0 + c * r1;
+        }
+        // (p, q) = (1, 2)
+        if (a12 != 0.0) {
+            const double th = (a22 - a11) / (2.0 * a12);
+            const double t = (th >= 0.0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
+            const double c = 1.0 / sqrt(t * t + 1.0), sn = t * c;
+            a11 -= t * a12; a22 += t * a12; a12 = 0.0;
+            const double r0 = a01, r1 = a02;
+            a01 = c * r0 - sn * r1; a02 = sn * r0 + c * r1;
+        }
+    }
+    double e0 = a00, e1 = a11, e2 = a22, t;
+    if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
+    if (e1 > e2) { t = e1; e1 = e2; e2 = t; }
+    if (e0 > e1) { t = e0; e0 = e1; e1 = t; }
+    lam[0] = e0; lam[1] = e1; lam[2] = e2;
+}
+
+// Ascending eigenvalues of a symmetric 3x3 matrix in FP64, replacing LAPACK
+// eigvals(Symmetric) (RadialShell.jl:215-220).  E = (11, 22, 33, 12, 13, 23).  The
+// trigonometric solution of the characteristic cubic (O. K. Smith, Comm. ACM 4(4):168,
+// 1961) is used where its angle is well conditioned; near a double eigenvalue (|r| close
+// to 1, where acos amplifies the rounding of r by 1 / sqrt(1 - r^2)) the Jacobi solver
+// above takes over, so the eigenvalue differences behind e_v and p_v keep full FP64
+// accuracy.
 __device__ __noinline__ void eig3(const double* E, double* lam) {
     const double a11 = E[0], a22 = E[1], a33 = E[2], a12 = E[3], a13 = E[4], a23 = E[5];
     const double q = (a11 + a22 + a33) / 3.0;
@@ -298,7 +346,7 @@ __device__ __noinline__ void eig3(const double* E, double* lam) {
     const double c12 = a12 * ip, c13 = a13 * ip, c23 = a23 * ip;
     double r = 0.5 * (c11 * (c22 * c33 - c23 * c23) - c12 * (c12 * c33 - c23 * c13) +
                       c13 * (c12 * c23 - c22 * c13));
-    r = fmin(1.0, fmax(-1.0, r));
+    if (fabs(r) > 1.0 - 1e-4) { eig3_jacobi(E, lam); return; }
     const double phi = acos(r) / 3.0;
     double e2 = q + 2.0 * pp * cos(phi);
     double e0 = q + 2.0 * pp * cos(phi + 2.0943951023931957);
@@ -1289,7 +1337,9 @@ constexpr size_t kStaticScratchBytes = 32u << 20;   // 32 MiB
 __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch per device, resolved once per device with that
-// device current (a host-side name of a __device__ array is not a device address).
+// device current (a host-side name of a __device__ array is not a device address).  The
+// address belongs to the device's primary context: after a cudaDeviceReset it is stale,
+// so the library must not be used across a reset of a device it has run on.
 constexpr int kMaxDevices = 64;
 void* g_static_addr[kMaxDevices] = {};
 std::mutex g_static_mu;
@@ -1356,6 +1406,7 @@ extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
     int bpsm = 0;
     rc = walk_blocks_per_sm<false>(&bpsm);
     if (rc != HT_OK) return rc;
+    if (ctx->tune_walk_bpsm > 0 && ctx->tune_walk_bpsm < bpsm) bpsm = ctx->tune_walk_bpsm;
     long long blocks = (long long)ctx->num_sms * bpsm;
     const long long fit = (long long)(kStaticScratchBytes / per_block);
     const long long items = (b->npeaks + kPeaksPerItem - 1) / kPeaksPerItem;

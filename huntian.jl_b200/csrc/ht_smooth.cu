@@ -658,7 +658,7 @@ template <int T, class Sh>
 __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     const float2* __restrict__ P, float2* __restrict__ B, int NK, int zlo, int Rz,
     const float* __restrict__ tab, const float2* __restrict__ twL,
-    const float2* __restrict__ tw32, int32_t* __restrict__ status) {
+    const float2* __restrict__ tw32, int32_t* __restrict__ status, long long wait_ns) {
     constexpr int COLS = Sh::cols, N = 32 * T, S = pencil_stride<T, COLS>(), NB = N / COLS,
                   H = T / 2;
     extern __shared__ __align__(128) float2 sm[];
@@ -701,7 +701,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
             wl[t] = __ldg(tab + (base + kz * kz));
         }
         const float wmid = __ldg(tab + (base + (N / 2) * (N / 2)));
-        ok = tid == 0 ? htasync::bar_wait(&bar, parity) : true;
+        ok = tid == 0 ? htasync::bar_wait(&bar, parity, wait_ns) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
             break;
@@ -746,7 +746,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     if (!ok && tid == 0) {
         // record the timeout, then wait (bounded) for the copy still in flight
         atomicExch(status, 1);
-        htasync::bar_wait(&bar, parity);
+        htasync::bar_wait(&bar, parity, wait_ns);
     }
 }
 
@@ -754,7 +754,7 @@ template <int T, class Sh>
 __global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
     const float2* __restrict__ B, float2* __restrict__ C, int NK, int NKP, int Rz, int ylo,
     int Ry, const float2* __restrict__ twL, const float2* __restrict__ tw32,
-    int32_t* __restrict__ status) {
+    int32_t* __restrict__ status, long long wait_ns) {
     constexpr int COLS = Sh::cols, N = 32 * T, S = pencil_stride<T, COLS>();
     extern __shared__ __align__(128) float2 sm[];
     float2* in = sm;
@@ -785,7 +785,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
     for (; task < ntasks; task += gridDim.x) {
         const int zr = task / NKB, kx0 = (task - zr * NKB) * COLS;
         const int ncol = min(COLS, NK - kx0);
-        ok = tid == 0 ? htasync::bar_wait(&bar, parity) : true;
+        ok = tid == 0 ? htasync::bar_wait(&bar, parity, wait_ns) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
             break;
@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
     }
     if (!ok && tid == 0) {
         atomicExch(status, 1);
-        htasync::bar_wait(&bar, parity);
+        htasync::bar_wait(&bar, parity, wait_ns);
     }
 }
 
@@ -833,7 +833,8 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
                                                  const float2* __restrict__ twp,
                                                  const float2* __restrict__ twM,
                                                  const float2* __restrict__ tw32,
-                                                 int32_t* __restrict__ status) {
+                                                 int32_t* __restrict__ status,
+                                                 long long wait_ns) {
     constexpr int M = 32 * TH, N = 2 * M, S = pencil_slot_x<TH>();
     static_assert(S >= pencil_row_pitch(N) && S >= 33 * TH, "a padded C row must fit a slot");
     extern __shared__ __align__(128) float2 sm[];
@@ -866,7 +867,7 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
             htasync::bulk_load(slots + (s ^ 1) * S, C + (r + stride) * NKP, row_bytes,
                                &bar[s ^ 1]);
         }
-        ok = lane == 0 ? htasync::bar_wait(&bar[s], (unsigned)((i >> 1) & 1)) : true;
+        ok = lane == 0 ? htasync::bar_wait(&bar[s], (unsigned)((i >> 1) & 1), wait_ns) : true;
         __syncwarp();
         if (__any_sync(0xffffffffu, !ok)) {
             ok = false;
@@ -901,9 +902,9 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
     if (!ok && lane == 0) {
         // record the timeout, then wait (bounded) for this warp's copies in flight
         atomicExch(status, 1);
-        htasync::bar_wait(&bar[i & 1], (unsigned)((i >> 1) & 1));
+        htasync::bar_wait(&bar[i & 1], (unsigned)((i >> 1) & 1), wait_ns);
         if (r + stride < rows)
-            htasync::bar_wait(&bar[(i & 1) ^ 1], (unsigned)(((i + 1) >> 1) & 1));
+            htasync::bar_wait(&bar[(i & 1) ^ 1], (unsigned)(((i + 1) >> 1) & 1), wait_ns);
     }
 }
 
@@ -940,13 +941,14 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
     const unsigned gy = (unsigned)std::min(yt, sms * by);
     const unsigned gx = (unsigned)std::min((rows + 7) / 8, sms * bx);
     pz_kernel<T, PencilZ><<<gz, PencilZ::threads, smz, st>>>(
-        P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL, tw.w32, status);
+        P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL, tw.w32, status, ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
     py_kernel<T, PencilY><<<gy, PencilY::threads, smy, st>>>(B, C, nk, nkp, Rz, ylo, Ry,
-                                                             tw.lmL, tw.w32, status);
+                                                             tw.lmL, tw.w32, status,
+                                                             ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
     px_kernel<TH><<<gx, 256, smx, st>>>(C, d_out, nkp, zlo, ylo, Ry, rows, tw.nat, tw.lmM,
-                                        tw.w32, status);
+                                        tw.w32, status, ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "px_kernel launch");
     return HT_OK;
 }

@@ -311,11 +311,15 @@ class HaloFinder:
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
 
     def tune(self, block_bits: Optional[int] = None, pf_kz: Optional[int] = None,
-             walk_bpsm: Optional[int] = None, fft_path: Optional[int] = None) -> None:
-        """Set launch parameters (ht_ctx_tune); all but fft_path are result-neutral."""
+             walk_bpsm: Optional[int] = None, fft_path: Optional[int] = None,
+             wait_ns: Optional[int] = None, inject_tx: Optional[int] = None) -> None:
+        """Set launch parameters (ht_ctx_tune); block_bits, pf_kz and walk_bpsm are
+        result-neutral.  wait_ns is the limit of the bounded in-kernel waits; inject_tx is
+        the test hook that makes the peak scan's first waits run out (0 = off)."""
         L = _lib.load()
         for key, v in ((_lib.HT_TUNE_BLOCK_BITS, block_bits), (_lib.HT_TUNE_PF_KZ, pf_kz),
-                       (_lib.HT_TUNE_WALK_BPSM, walk_bpsm), (_lib.HT_TUNE_FFT_PATH, fft_path)):
+                       (_lib.HT_TUNE_WALK_BPSM, walk_bpsm), (_lib.HT_TUNE_FFT_PATH, fft_path),
+                       (_lib.HT_TUNE_WAIT_NS, wait_ns), (_lib.HT_TUNE_INJECT_TX, inject_tx)):
             if v is not None:
                 check(L.ht_ctx_tune(self._h, key, int(v)))
 
@@ -328,6 +332,43 @@ class HaloFinder:
 
 
 # ----------------------------------------------------------- reference mirrors ----
+
+@dataclass
+class ShellTables:
+    """ShellAnalysisGPU.ShellTables (src/ShellAnalysisGPU.jl:28-36): the r^2-sorted cell
+    offsets grouped into shells, 1-based shell_start like the reference's."""
+    offsets_di: np.ndarray
+    offsets_dj: np.ndarray
+    offsets_dk: np.ndarray
+    shell_start: np.ndarray
+    shell_count: np.ndarray
+    shell_r2: np.ndarray
+    nshells: int
+
+    @property
+    def rmax(self) -> int:
+        """The hunt radius the tables were built for (largest r with r^2 in the table)."""
+        return math.isqrt(int(self.shell_r2[-1])) if self.nshells else 0
+
+
+def build_shell_tables(rmax: int) -> ShellTables:
+    """ShellAnalysisGPU.build_shell_tables (src/ShellAnalysisGPU.jl:44-71) over
+    RadialShell.precompute_shells (src/HaloFinder/RadialShell.jl:151-166): every offset
+    with r^2 <= rmax^2, generated dk-outer, dj, di-inner and stably sorted by r^2."""
+    r = np.arange(-rmax, rmax + 1, dtype=np.int32)
+    dk, dj, di = np.meshgrid(r, r, r, indexing="ij")   # di fastest, as the loops nest
+    di, dj, dk = di.ravel(), dj.ravel(), dk.ravel()
+    r2 = di * di + dj * dj + dk * dk
+    keep = r2 <= rmax * rmax
+    di, dj, dk, r2 = di[keep], dj[keep], dk[keep], r2[keep]
+    o = np.argsort(r2, kind="stable")
+    di, dj, dk, r2 = di[o], dj[o], dk[o], r2[o]
+    edges = np.flatnonzero(np.diff(r2)) + 1
+    start0 = np.concatenate([[0], edges]).astype(np.int64)
+    count = np.diff(np.concatenate([start0, [len(r2)]])).astype(np.int64)
+    return ShellTables(di.astype(np.int32), dj.astype(np.int32), dk.astype(np.int32),
+                       start0 + 1, count, r2[start0].astype(np.int32), int(len(start0)))
+
 
 @dataclass
 class PeakCandidate:
@@ -418,12 +459,17 @@ def analyse_peaks_gpu_cuda_multirf(delta, etax, etay, etaz, eta2x, eta2y, eta2z,
     """Mirror of `analyse_peaks_gpu_cuda_multirf` (ext/CUDAExt.jl:2085-2344).
 
     `batches` are (peaks_i, peaks_j, peaks_k, Rf, ir2min[, ZZon_pp, fcrit_pp]) tuples;
-    `stab` is the hunt radius (int) or an object with `.rmax`.  All batches go to the
-    library in ONE launch.  Returns (results, mask): a list with one dict of the 14
+    `stab` is a ShellTables (build_shell_tables, the reference's type) or the hunt radius
+    as an int.  All batches go to the library in ONE launch.  Returns (results, mask): a list with one dict of the 14
     output arrays per batch (host numpy, reference shapes (3, n) / (3, 3, n)), and the
     updated mask (numpy) or None.  Device-resident inputs are used in place."""
     device = device or torch.device("cuda", torch.cuda.current_device())
-    nhunt = stab if isinstance(stab, (int, np.integer)) else int(stab.rmax)
+    if isinstance(stab, (int, np.integer)):
+        nhunt = int(stab)
+    elif isinstance(stab, ShellTables):
+        nhunt = stab.rmax
+    else:
+        raise TypeError("stab must be a ShellTables (build_shell_tables) or an int hunt radius")
     if finder is None or finder.nhunt != nhunt:
         finder = HaloFinder(nhunt, ct_table, X1, X2, Y1, Y2, Z1, Z2, out_val=ct_out_val,
                             device=device.index or 0)

@@ -285,8 +285,9 @@ HT_API int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* batch, double alat
  * ht_shell_analyse's.
  *
  * - The first call on a device resolves the array's device address
- *   (cudaGetSymbolAddress) with that device current; make that first call before any
- *   stream capture begins.
+ *   (cudaGetSymbolAddress) with that device current and keeps it for the life of the
+ *   process; make that first call before any stream capture begins, and do not use the
+ *   library across a cudaDeviceReset of that device (the kept address would be stale).
  * - All calls share the one array: calls whose kernels overlap on the GPU (e.g. on two
  *   streams, or from two threads) race on it and give wrong results.  Serialize them.
  * - Limit: one 8-warp block's scratch, 8 warps * 4 peak slots * (nshells + 2) * 128 bytes,
@@ -315,6 +316,18 @@ HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* fields,
 #define HT_TUNE_PF_KZ 2
 #define HT_TUNE_WALK_BPSM 3
 #define HT_TUNE_FFT_PATH 4
+/* Two more keys set the bounded in-kernel waits (the TMA pipelines of the peak scan and of
+ * the pencil smoothing), which give up instead of hanging and report through
+ * ht_device_status:
+ *   HT_TUNE_WAIT_NS     the limit of every wait, in ns of %globaltimer (1e3 .. 6e10;
+ *                       default 2e9);
+ *   HT_TUNE_INJECT_TX   test hook (default 0): every peak-scan CTA announces this many bytes
+ *                       (a multiple of 16, at most 4096) beyond its first copy, so its first
+ *                       wait runs out although the copy itself completes; the scan then
+ *                       records status 1, drains its copies and returns, and its peaks are
+ *                       invalid.  Nothing faults or hangs; set it back to 0 to scan again. */
+#define HT_TUNE_WAIT_NS 5
+#define HT_TUNE_INJECT_TX 6
 HT_API int ht_ctx_tune(ht_ctx* ctx, int32_t key, int64_t value);
 
 /* ------------------------------------------------ lightcone and halo records ---- */

@@ -62,7 +62,9 @@ class Grid(C.Structure):
 
 RESULT_FIELDS = [("RTHL", 1), ("Srb", 1), ("Sbar", 3), ("Sbar2", 3), ("strain", 9),
                  ("gradpk", 3), ("gradpkrf", 3), ("Fbarx", 1), ("e_v", 1), ("p_v", 1),
-                 ("zvir_half", 1), ("gradpkf", 3), ("d2F", 1), ("eigs", 3)]
+                 ("zvir_half", 1), ("gradpkf", 3), ("d2F", 1), ("eigs", 3),
+                 # diagnostic: smallest |Fbar - fcrit| / |zvir - ZZon| of the decisions
+                 ("margin", 1)]
 RESULT_DTYPE = np.dtype([(n, np.float64) if k == 1 else (n, np.float64, (k,))
                          for n, k in RESULT_FIELDS])
 
@@ -95,6 +97,7 @@ def _declare(L):
                                    C.c_double, C.POINTER(CTab), _P, C.c_int64, C.c_int,
                                    C.c_double, C.c_int, _P, _P, C.c_int]
     L.or_max_threads.restype = C.c_int
+    L.or_set_exact_products.argtypes = [C.c_int]
 
 
 def _ptr(a):
@@ -235,8 +238,11 @@ def analyse_peak(fields: Fields, ipp: int, alatt: float, ir2min: int, ZZon: floa
 
 def analyse_batch(fields: Fields, pi, pj, pk, ir2min, Rf, ZZon, fcrit, alatt: float,
                   ct: CollapseTable, shells: np.ndarray, *, nbuff: int = 0,
-                  rmax2rs: float = 0.0, kind: str = "cudakernel", nthreads: int = 0):
-    """Many peaks on all host threads.  Per-peak arrays; fcrit < 0 means fsc_of_z."""
+                  rmax2rs: float = 0.0, kind: str = "cudakernel", nthreads: int = 0,
+                  exact_products: bool = False):
+    """Many peaks on all host threads.  Per-peak arrays; fcrit < 0 means fsc_of_z.
+    exact_products: form every cell product in Float64 (the full-FP64 oracle) instead of
+    rounding it to Float32 as the reference does."""
     n = len(pi)
     a32 = lambda v: np.ascontiguousarray(np.broadcast_to(v, (n,)), dtype=np.int32)
     a64 = lambda v: np.ascontiguousarray(np.broadcast_to(v, (n,)), dtype=np.float64)
@@ -245,11 +251,13 @@ def analyse_batch(fields: Fields, pi, pj, pk, ir2min, Rf, ZZon, fcrit, alatt: fl
     out = np.zeros(n, dtype=RESULT_DTYPE)
     codes = np.zeros(n, dtype=np.int32)
     cells = np.ascontiguousarray(shells, dtype=np.int32)
+    lib().or_set_exact_products(1 if exact_products else 0)
     lib().or_analyse_batch(fields.c, n, pi.ctypes.data, pj.ctypes.data, pk.ctypes.data,
                            ir2.ctypes.data, Rf.ctypes.data, ZZon.ctypes.data,
                            fcrit.ctypes.data, alatt, ct.c, cells.ctypes.data, len(cells),
                            nbuff, rmax2rs, KIND[kind], out.ctypes.data, codes.ctypes.data,
                            nthreads)
+    lib().or_set_exact_products(0)
     return out, codes
 
 

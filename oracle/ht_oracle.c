@@ -354,11 +354,37 @@ static void ev_pv(const double E[9], double* Frho, double* e_v, double* p_v, dou
     if (lam_out) { lam_out[0] = lam[0]; lam_out[1] = lam[1]; lam_out[2] = lam[2]; }
 }
 
+/* Product of a Float32 field value and an integer offset as the reference forms it:
+ * Float32 * Int32 is Float32 in Julia, so every cell product is rounded to Float32 before
+ * it enters the Float64 shell sum (RadialShell.jl:437-443, ShellAnalysisGPU.jl:205-215).
+ * With exact products on (or_set_exact_products) the product is formed in Float64, where
+ * it is exact: the "full-FP64" variant of the oracle, whose difference from the default
+ * is the reference's own rounding noise. */
+static int g_exact_products = 0;
+
+void or_set_exact_products(int on) { g_exact_products = on != 0; }
+
+static inline double cell_product(float v, int32_t d)
+{
+    return g_exact_products ? (double)v * (double)d : (double)(float)(v * (float)d);
+}
+
 static void set_no_collapse(or_result* r)
 {
     memset(r, 0, sizeof(*r));
     r->RTHL = -1.0;
     r->zvir_half = -1.0;
+    r->margin = INFINITY;
+}
+
+/* Smallest |value - threshold| over the collapse-deciding comparisons of one peak (the
+ * Fbar-vs-fcrit tests of the crossing search and the zvir-vs-ZZon tests of the inward
+ * walk): a diagnostic for collapse flips against another implementation, not a
+ * reference output. */
+static void note_margin(double* margin, double diff)
+{
+    const double d = fabs(diff);
+    if (d < *margin) *margin = d;
 }
 
 /* Shared tail of analyse_peak / analyse_peak_gpu once the profiles exist:
@@ -391,10 +417,14 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
     kernel_strain(P, mrf, mlow_rf, mupp_rf, wRnor, aRnor, E, gradpkrf, gf1);
 
     /* crossing (RadialShell.jl:485-526) */
+    double margin = INFINITY;
+    note_margin(&margin, P->Fbar[m0] - fcrit);
     if (P->Fbar[m0] >= fcrit) {
         int found = 0;
-        for (int64_t mm = m0; mm <= m; ++mm)
+        for (int64_t mm = m0; mm <= m; ++mm) {
+            note_margin(&margin, P->Fbar[mm] - fcrit);
             if (P->Fbar[mm] < fcrit) { m0 = mm; found = 1; break; }
+        }
         if (!found) mupp = m;
         if (found) {
             double rupp_m0 = P->rad[m0] + 2.0;
@@ -405,10 +435,11 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
         int64_t mstart = m0 - 1 > 1 ? m0 - 1 : 1;
         int found = 0;
         for (int64_t mp = mstart; mp >= 1; --mp) {
+            note_margin(&margin, P->Fbar[mp] - fcrit);
             if (P->Fbar[mp] >= fcrit) { found = 1; break; }
             m0 = mp;
         }
-        if (!found) { set_no_collapse(out); return 2; }
+        if (!found) { set_no_collapse(out); out->margin = margin; return 2; }
         double rupp_m0 = P->rad[m0] + 2.0;
         int64_t mupp_new = m0;
         for (int64_t mm = m0 + 1; mm <= m; ++mm) if (P->rad[mm] < rupp_m0) mupp_new = mm;
@@ -443,7 +474,7 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
         zvir1 = -1.0; zvir1p = zvir1p_m0; collapsed = 1;
     } else {
         zvir1 = zvir1p_m0;
-        if (m0 == 1) { set_no_collapse(out); return 3; }
+        if (m0 == 1) { set_no_collapse(out); out->margin = margin; return 3; }
         for (int64_t mp = m0 - 1; mp >= 1; --mp) {
             double rupp_mp = P->rad[mp] + 2.0;
             double rlow_mp = fmax(P->rad[mp] - 2.0, 0.0);
@@ -467,6 +498,7 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
             if (Frho_mp > 0.0) {
                 double poe = e_v_mp < 1e-5 ? 0.0 : p_v_mp / e_v_mp;
                 zvir1p_mp = or_interp(ct, log10(Frho_mp), e_v_mp, poe);
+                note_margin(&margin, zvir1p_mp - ZZon);
             }
             if (zvir1p_mp >= ZZon) {
                 m0 = mp + 1;
@@ -488,7 +520,7 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
     }
     /* Frhpk..Fpvpk, Frho, e_v, p_v are carried as in the reference but unused there */
     (void)Frhpk; (void)Fnupk; (void)Fevpk; (void)Fpvpk; (void)Frho; (void)e_v; (void)p_v;
-    if (!collapsed) { set_no_collapse(out); return 4; }
+    if (!collapsed) { set_no_collapse(out); out->margin = margin; return 4; }
 
     /* RTHL (RadialShell.jl:689-700) */
     double dZvir = zvir1p - zvir1, RTHL;
@@ -499,7 +531,7 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
     } else {
         RTHL = rp;
     }
-    if (!(RTHL > 0.0)) { set_no_collapse(out); return 5; }
+    if (!(RTHL > 0.0)) { set_no_collapse(out); out->margin = margin; return 5; }
 
     double RTHL3 = RTHL * RTHL * RTHL;
     double RTHL5 = RTHL3 * RTHL * RTHL;
@@ -653,6 +685,7 @@ static int tail(const walk_ctx* W, prof_t* P, int64_t m, int64_t m0, int64_t mup
         out->gradpkf[i] = gpkf[i]; out->gradpkrf[i] = gradpkrf[i]; out->eigs[i] = lamf[i];
     }
     memcpy(out->strain, strain_final, sizeof strain_final);
+    out->margin = margin;
     return 0;
 }
 
@@ -757,9 +790,9 @@ int or_analyse_peak(const or_grid* g, int64_t ipp, double alatt, int ir2min, dou
         for (int L = 0; L < 3; ++L) {
             P.S[L][m + 1] += (double)ev[L];
             P.S2[L][m + 1] += (double)e2[L];
-            P.G[L][m + 1] += (double)(float)(dv * (float)ix[L]);
-            P.Gf[L][m + 1] += (double)(float)(dT * (float)ix[L]);
-            for (int K = 0; K < 3; ++K) P.SR[L][K][m + 1] += (double)(float)(ev[L] * (float)ix[K]);
+            P.G[L][m + 1] += cell_product(dv, ix[L]);
+            P.Gf[L][m + 1] += cell_product(dT, ix[L]);
+            for (int K = 0; K < 3; ++K) P.SR[L][K][m + 1] += cell_product(ev[L], ix[K]);
         }
     }
 
@@ -857,9 +890,9 @@ static int analyse_gpu_impl(const or_grid* g, int64_t ipp, double alatt, int ir2
                         float e2 = L == 0 ? g->eta2x[cv] : L == 1 ? g->eta2y[cv] : g->eta2z[cv];
                         lS2[L] += (double)e2;
                     }
-                    lG[L] += (double)(float)(dv * (float)ix[L]);
-                    lGf[L] += (double)(float)(dT * (float)ix[L]);
-                    for (int K = 0; K < 3; ++K) lSR[L][K] += (double)(float)(ev[L] * (float)ix[K]);
+                    lG[L] += cell_product(dv, ix[L]);
+                    lGf[L] += cell_product(dT, ix[L]);
+                    for (int K = 0; K < 3; ++K) lSR[L][K] += cell_product(ev[L], ix[K]);
                 }
             }
             m += 1;

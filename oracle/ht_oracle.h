@@ -66,6 +66,9 @@ typedef struct {
 typedef struct {
     double RTHL, Srb, Sbar[3], Sbar2[3], strain[9], gradpk[3], gradpkrf[3];
     double Fbarx, e_v, p_v, zvir_half, gradpkf[3], d2F, eigs[3];
+    /* diagnostic, not a reference output: the smallest |Fbar - fcrit| or |zvir - ZZon|
+     * over the comparisons that decided the collapse (infinity when none did) */
+    double margin;
 } or_result;
 
 /* RadialShell.analyse_peak (RadialShell.jl:281-865), literal: per-cell shell walk, FP64.
@@ -96,6 +99,10 @@ void or_analyse_batch(const or_grid* g, int64_t npeaks, const int32_t* pi, const
                       int nthreads);
 
 int or_max_threads(void);
+
+/* 0 (default): cell products rounded to Float32 as the reference forms them; 1: products
+ * formed exactly in Float64 (the full-FP64 oracle).  Process-wide; set it between calls. */
+void or_set_exact_products(int on);
 
 /* ---- collapse-table generation (or_collapse.c) ---- */
 

@@ -86,3 +86,89 @@ def compare(gpu, ora, rel=1e-5, abs_floor=None):
         if worst:
             bad.append((p, worst))
     return bad, flips
+
+
+def make_box_workload(ht, n, L, nbuff, nf, rmin, rmax, seed, max_peaks=1 << 23):
+    """A periodic-box workload as the benchmark builds it: seeded BBKS Gaussian field with
+    2LPT displacements on an n^3 box (library-independent torch code), wrapped to an
+    (n + 2 nbuff)^3 tile; nf log-spaced top-hat filters R = rmin..rmax smoothed by the
+    library and scanned with the mask carried.  Returns a dict with the device tile, the
+    finder, the peaks and the per-peak filter parameters."""
+    import os
+    from huntian_b200 import synth
+    from conftest import GOLDEN
+    dev = torch.device("cuda", 0)
+    cosmo = synth.Cosmology()
+    dk = synth.gaussian_box(n, L, seed, cosmo, dev)
+    psi1, psi2 = synth.displacements(dk, n, L, ilpt=2)
+    tile = {"delta": synth.wrap_pad(synth._irfft(dk, n), nbuff)}
+    for nm, t in zip(("etax", "etay", "etaz", "eta2x", "eta2y", "eta2z"), psi1 + psi2):
+        tile[nm] = synth.wrap_pad(t, nbuff)
+    del dk, psi1, psi2
+    nt = n + 2 * nbuff
+    alatt = L / n
+    filters = ht.log_filterbank(nf, rmin, rmax)
+    tab, axes = ht.read_homeltab(os.path.join(GOLDEN, "HomelTab_julia.dat"))
+    finder = ht.HaloFinder(ht.nhunt_of(filters[0][2], alatt, nbuff), tab, *axes)
+    fcrit = float(np.float32(finder.fsc_of_z(0.0)))
+    mask = torch.zeros((nt,) * 3, dtype=torch.int8, device=dev)
+    peaks = ht.HaloFinder.alloc_peaks(max_peaks, dev, False)
+    delta_k = torch.fft.rfftn(tile["delta"], dim=(0, 1, 2)).contiguous()
+    ds = torch.empty((nt,) * 3, dtype=torch.float32, device=dev)
+    for fi, flt in enumerate(filters, start=1):
+        finder.smooth_tile(delta_k, nt, nt * alatt, flt[2], 1, out=ds)
+        finder.peakfind_filter(ds, mask, nbuff, fcrit, fi, max_peaks, peaks)
+    torch.cuda.synchronize()
+    del delta_k, ds
+    npk = int(peaks["count"].item())
+    fidx = peaks["filter_idx"][:npk].long() - 1
+    Rf_all = torch.tensor([f[2] for f in filters], dtype=torch.float64, device=dev)
+    ir2_all = torch.tensor([ht.ir2min_of(f[2], alatt) for f in filters], dtype=torch.int32,
+                           device=dev)
+    args = (peaks["i"][:npk], peaks["j"][:npk], peaks["k"][:npk], Rf_all[fidx], ir2_all[fidx],
+            torch.ones(npk, dtype=torch.float32, device=dev),
+            torch.full((npk,), fcrit, dtype=torch.float32, device=dev), alatt)
+    return {"tile": tile, "finder": finder, "peaks": peaks, "npk": npk, "filters": filters,
+            "alatt": alatt, "fcrit": fcrit, "tab": tab, "axes": axes, "nbuff": nbuff,
+            "fidx": fidx, "Rf_all": Rf_all, "ir2_all": ir2_all, "args": args}
+
+
+def oracle_sample(oracle, W, sel, kind, exact_products=False):
+    """Oracle results (and its time in seconds) for the peaks `sel` of a workload;
+    exact_products: the full-FP64 variant (cell products formed exactly)."""
+    import time
+    host = {k: v.cpu().numpy() for k, v in W["tile"].items()}
+    F = oracle.Fields(host["delta"], host["etax"], host["etay"], host["etaz"], host["eta2x"],
+                      host["eta2y"], host["eta2z"])
+    ct = oracle.CollapseTable(W["tab"], *W["axes"])
+    p = W["peaks"]
+    n = W["npk"]
+    pi, pj, pk = (p[c][:n].cpu().numpy()[sel] for c in ("i", "j", "k"))
+    fi = W["fidx"].cpu().numpy()[sel]
+    t0 = time.perf_counter()
+    o, _ = oracle.analyse_batch(F, pi, pj, pk, W["ir2_all"].cpu().numpy()[fi],
+                                W["Rf_all"].cpu().numpy()[fi], 1.0, np.float32(W["fcrit"]),
+                                W["alatt"], ct, oracle.precompute_shells(W["finder"].nhunt),
+                                nbuff=W["nbuff"], kind=kind, exact_products=exact_products)
+    return o, time.perf_counter() - t0
+
+
+def result_rows(ht, res, npk, sel):
+    """Per-peak rows of the selected peaks from the library's flat result arrays."""
+    width = ht.RESULT_WIDTH
+    g = {k: v.cpu().numpy() for k, v in res.items()}
+    return {k: g[k][:npk * width.get(k, 1)].reshape(npk, -1)[sel] for k in SCALAR + VECTOR}
+
+
+def print_report(rep, label):
+    print(f"\n{label}: {rep['peaks']} peaks, {rep['collapsed']} collapsed in both, "
+          f"{rep['flips']} flips ({rep['flips_unexplained']} above the margin), "
+          f"{rep['mismatches']} mismatches, {rep['within_reference_noise']} beyond 1e-5 "
+          f"within the reference's rounding noise")
+    print(f"{'field':10s} {'max rel err':>12s}")
+    for f, v in rep["max_rel"].items():
+        print(f"{f:10s} {v:12.3e}")
+    if rep["flip_list"]:
+        print("flips (peak, oracle decision margin):", rep["flip_list"])
+    if rep["mismatch_list"]:
+        print("mismatches (peak, field, rel err):", rep["mismatch_list"])

@@ -3,8 +3,11 @@
 Callers that cannot allocate device memory while they run this step (work issued into
 a stream under CUDA-graph capture, or a host that owns the device memory pool) use
 ht_shell_analyse_static, which keeps its scratch in a static array of the library.  It
-must give the same results as ht_shell_analyse, on two calls in a row (the static array
-keeps the previous call's contents).  This file is collected last on purpose.
+must give the same results as ht_shell_analyse, bit for bit (both run the same walk over
+the fields in place), on two calls in a row (the static array keeps the previous call's
+contents); its results must agree with the oracle (oracle/parity.py), and the second call
+must leave the device's free memory unchanged (the first call of a process may load the
+library's device code and array).  This file is collected last on purpose.
 """
 import numpy as np
 import pytest
@@ -52,16 +55,31 @@ def test_static_scratch_matches_allocating_entry(ht, oracle, julia_table_path):
         out = ht.HaloFinder.alloc_results(npk, "cuda")
         for v in out.values():
             v.fill_(float("nan"))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         finder.analyse_static(fields, *args, nbuff=2, mask=mask_b, out=out)
         torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
+        if call == 1:
+            assert free1 == free0, (free0, free1)
         for name in ht.RESULT_NAMES:
-            a = ref[name].cpu().numpy()
-            b = out[name].cpu().numpy()
             w = ht.RESULT_WIDTH.get(name, 1)
-            a, b = a[:npk * w], b[:npk * w]
-            both_nan = np.isnan(a) & np.isnan(b)
-            scale = np.maximum(np.abs(a), 1e-4)
-            assert np.all(both_nan | (np.abs(a - b) <= 1e-5 * scale)), (call, name)
+            a = ref[name][:npk * w].view(torch.int32)
+            b = out[name][:npk * w].view(torch.int32)
+            assert torch.equal(a, b), (call, name)
         assert torch.equal(mask_a, mask_b), call
         assert (ref["RTHL"][:npk] > 0).any()
+        # and the oracle (the reference's GPU-entry semantics, full-FP64 noise reference)
+        from oracle import parity
+        F = oracle.Fields(d, *eta[:3], *eta[3:], lapd=lapd)
+        kw = dict(nbuff=2, kind="cudakernel")
+        shells = oracle.precompute_shells(12)
+        ct = oracle.read_homeltab(julia_table_path)
+        ora_args = (F, i, j, k, 12, 3.0, 1.0, np.float32(1.3), 1.5, ct, shells)
+        ox, _ = oracle.analyse_batch(*ora_args, exact_products=True, **kw)
+        o, _ = oracle.analyse_batch(*ora_args, **kw)
+        g = {n: out[n][:npk * ht.RESULT_WIDTH.get(n, 1)].cpu().numpy()
+             .reshape(npk, -1) for n in ht.RESULT_NAMES}
+        rep = parity.report(g, o, ora_exact=ox)
+        assert rep["mismatches"] == 0 and rep["flips_unexplained"] == 0, rep
     finder.close()
