@@ -273,7 +273,6 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
     for (size_t m = 0; m < rad.size(); ++m)
         if (rad[m] > 0.0) { irad[m] = 1.0 / rad[m]; irad3[m] = 1.0 / (rad[m] * rad[m] * rad[m]); }
     c->nweights = (int64_t)wm1.size();
-    if (const char* v = getenv("HT_SMALL_MAX_SHELLS")) c->small_max_shells = atoi(v);
     int rc;
     if ((rc = upload(&c->d_off, c->h_off.data(), c->h_off.size(), "shell offsets")) ||
         (rc = upload(&c->d_start, c->h_start.data(), c->h_start.size(), "shell starts")) ||

@@ -38,8 +38,6 @@ struct ht_ctx {
     int32_t* d_wrow = nullptr;     // [nshells + 2]
     int32_t* d_wm1 = nullptr;
     double* d_wwt = nullptr;
-    // peaks whose minimum walk spans at most this many shells run 8 lanes per peak
-    int small_max_shells = 96;
     // result-neutral tunables (ht_ctx_tune)
     int tune_block_bits = 17;      // LEARNED order: spatial block of 2^bits cells
     int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)

@@ -1,9 +1,8 @@
 // Radial-shell collapse on sm_100a.
 //
-// A peak is handled by a group of G lanes of one warp: G = 8 for peaks whose walk is
-// short (four peaks share a warp), G = 32 for the rest.  G is a pure function of the
-// peak's own filter radius and ir2min, so every execution mode gives bit-identical
-// results.  For each peak the group walks the shells of the r^2-sorted offset table
+// A peak is handled by a group of G = 8 lanes of one warp (four peaks share a warp; on
+// the benchmark tiles this beat 32 lanes per peak for the long walks as well as for the
+// short ones).  For each peak the group walks the shells of the r^2-sorted offset table
 // outward (the per-shell gather of ShellAnalysisGPU.jl:153-229 / ext/CUDAExt.jl:752-924):
 // each lane accumulates 13 sums per shell in FP64 from the FP32 cell values (delta,
 // delta*d, delta^T*d, and the symmetrised strain psi_L d_K + psi_K d_L, every product
@@ -37,8 +36,8 @@ namespace {
 constexpr int kWarpsPerBlock = 8;
 constexpr int kThreads = kWarpsPerBlock * 32;
 constexpr int kRec = 16;          // doubles per shell in the scratch profile
-constexpr int kPeaksPerItem = 4;  // consecutive peaks per work item
-constexpr int kSmallG = 8;        // lanes per peak for short walks
+constexpr int kSmallG = 8;        // lanes per peak
+constexpr int kPeaksPerItem = 32 / kSmallG;  // peaks per work item (one per group)
 
 // Scratch profile record, one per shell m (1-based):
 enum : int {
@@ -54,14 +53,11 @@ enum : int { V_F = 0, V_N = 1, V_G = 2, V_GF = 5, V_SR = 8, V_ROWS = 14 };
 
 // Shared-memory staging per group: [V_ROWS][G + 1] doubles for the shell sums (the last
 // column holds the totals), or [G + 1][kStepW] doubles for inward-walk steps.
-constexpr int kStepW = 16;
+constexpr int kStepW = 14;
 __host__ __device__ constexpr int group_smem_doubles(int G) {
     return V_ROWS * (G + 1) > (G + 1) * kStepW ? V_ROWS * (G + 1) : (G + 1) * kStepW;
 }
-constexpr int kWarpSmemDoubles =
-    group_smem_doubles(32) > (32 / kSmallG) * group_smem_doubles(kSmallG)
-        ? group_smem_doubles(32)
-        : (32 / kSmallG) * group_smem_doubles(kSmallG);
+constexpr int kWarpSmemDoubles = kPeaksPerItem * group_smem_doubles(kSmallG);
 
 struct WalkArgs {
     const float4* rec;
@@ -110,7 +106,6 @@ struct WalkArgs {
     double zh_frac[10];     // cbrt(0.5 + 0.5 jj / 9), jj = 0..9 (zvir_half radii)
     int nbuff;
     int conv;
-    int small_max_shells;   // peaks whose minimum walk is <= this use G = 8
     int block_bits;         // LEARNED order: Morton block of 2^block_bits cells
     int8_t* mask;
     ht_results out;
@@ -450,12 +445,14 @@ struct CellLoader;
 
 template <>
 struct CellLoader<true> {
-    __device__ __forceinline__ static void load(const WalkArgs& a, long long idx, int iv1,
-                                                int iv2, int iv3, float (&v)[8]) {
-        const float4 x = __ldg(a.rec + 2 * idx);
-        const float4 y = __ldg(a.rec + 2 * idx + 1);
-        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-        v[4] = y.x; v[5] = y.y; v[6] = y.z; v[7] = y.w;
+    // the cell's 32-byte record in one 256-bit load (records are 32-byte aligned): one
+    // L1 request per cell instead of two
+    __device__ __forceinline__ static void load(const WalkArgs& a, long long idx, int, int,
+                                                int, float (&v)[8]) {
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+              "=f"(v[6]), "=f"(v[7])
+            : "l"(a.rec + 2 * idx));
     }
 };
 
@@ -566,22 +563,12 @@ __device__ __forceinline__ Bounds peak_bounds(const WalkArgs& a, double Rf, int 
     return b;
 }
 
-// G = 8 for peaks whose data-independent minimum walk (to the first shell past ir2min
-// and the window of mrf) has at most small_max_shells shells, else 32.
-__device__ __forceinline__ int group_size_of(const WalkArgs& a, const Bounds& b) {
-    return max(b.m0_init, b.need_rf) <= a.small_max_shells ? kSmallG : 32;
-}
-
 __device__ __forceinline__ Bounds bounds_of(const WalkArgs& a, long long p) {
     if (a.bounds) {
         const int4 v = __ldg(a.bounds + p);
         return Bounds{v.x, v.y, v.z, v.w};
     }
     return peak_bounds(a, a.Rf[p], a.ir2min[p]);
-}
-
-__device__ __forceinline__ int group_size(const WalkArgs& a, long long p) {
-    return group_size_of(a, bounds_of(a, p));
 }
 
 template <bool PACKED>
@@ -632,9 +619,11 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
             acc[1].add_prod(v[0], d0); acc[2].add_prod(v[0], d1); acc[3].add_prod(v[0], d2);
             acc[4].add_prod(v[1], d0); acc[5].add_prod(v[1], d1); acc[6].add_prod(v[1], d2);
             const float e0 = v[2], e1 = v[3], e2 = v[4];
-            acc[7].add_prod(2.0f * e0, d0);
-            acc[8].add_prod(2.0f * e1, d1);
-            acc[9].add_prod(2.0f * e2, d2);
+            // the diagonal strain sums psi_L d_L are doubled when the shell is finalised
+            // (doubling commutes with the rounding of every product and sum)
+            acc[7].add_prod(e0, d0);
+            acc[8].add_prod(e1, d1);
+            acc[9].add_prod(e2, d2);
             acc[10].add_prod(e0, d1); acc[10].add_prod(e1, d0);
             acc[11].add_prod(e0, d2); acc[11].add_prod(e2, d0);
             acc[12].add_prod(e1, d2); acc[12].add_prod(e2, d1);
@@ -665,6 +654,7 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
             double v;
             if (i == P_FBAR) v = Fbar_s;
             else if (i == P_CSRB) v = csrb;
+            else if (i >= P_SR && i < P_SR + 3) v = (2.0 * R[(V_G + i - P_G) * RP + G]) * a.irad[s];
             else v = R[(V_G + i - P_G) * RP + G] * a.irad[s];   // G, Gf, SR rows in order
             q[i] = v;
         }
@@ -976,63 +966,22 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
     }
 }
 
-// One work item: kPeaksPerItem consecutive peaks.  If all of them take G = 8, four
-// groups of 8 lanes run them side by side; otherwise they run one after the other, each
-// with its own G (lanes 8..31 idle for a G = 8 peak).  Group q of warp w owns scratch
-// slot 4 w + q.
+// One work item: kPeaksPerItem consecutive entries of the processing order, one per
+// group of kSmallG lanes; group q of warp w owns scratch slot kPeaksPerItem w + q.
 template <bool PACKED>
 __device__ __forceinline__ void process_item(const WalkArgs& a, long long item, double* P0,
                                              double* W, int lane) {
-    const long long p0 = item * kPeaksPerItem;
-    const int np = (int)min((long long)kPeaksPerItem, a.npeaks - p0);
-    long long pid[kPeaksPerItem];
-    int gs[kPeaksPerItem];
-    bool all_small = np == kPeaksPerItem;
-#pragma unroll
-    for (int k = 0; k < kPeaksPerItem; ++k) {
-        long long p = p0 + k;
-        if (k < np && a.order) {
-            p = (long long)__ldg(a.order + p);
-            if (p < 0 || p >= a.npeaks) p = -1;   // not a peak index: skipped
-        }
-        pid[k] = k < np ? p : -1;
-        gs[k] = pid[k] >= 0 ? group_size(a, pid[k]) : 0;
-        all_small = all_small && gs[k] == kSmallG;
+    const int q = lane / kSmallG;
+    const long long e = item * kPeaksPerItem + q;
+    long long p = -1;
+    if (e < a.npeaks) {
+        p = a.order ? (long long)__ldg(a.order + e) : e;
+        if (p < 0 || p >= a.npeaks) p = -1;   // not a peak index: skipped
     }
-    // pid[i] / gs[i] for a run-time i, by selects (no local-memory array)
-    auto pick = [&](int i, long long& p, int& G) {
-        p = pid[0];
-        G = gs[0];
-#pragma unroll
-        for (int k = 1; k < kPeaksPerItem; ++k)
-            if (i == k) { p = pid[k]; G = gs[k]; }
-    };
-    // one call site of process_peak: four groups of 8 side by side, or the peaks one after
-    // the other with their own G
-    const int rounds = all_small ? 1 : np;
-    for (int k = 0; k < rounds; ++k) {
-        long long p;
-        int G;
-        Group g;
-        double* Pq = P0;
-        double* Wq = W;
-        bool run;
-        if (all_small) {
-            const int q = lane / kSmallG;
-            pick(q, p, G);
-            g = Group{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
-            Pq = P0 + q * a.scratch_stride;
-            Wq = W + q * group_smem_doubles(kSmallG);
-            run = true;
-        } else {
-            pick(k, p, G);
-            g = G == 32 ? Group{32, lane, 0, 0xffffffffu}
-                        : Group{kSmallG, lane, 0, (1u << kSmallG) - 1u};
-            run = G == 32 || (G == kSmallG && lane < kSmallG);
-        }
-        if (run) process_peak<PACKED>(a, p, Pq, Wq, g);
-        __syncwarp();
-    }
+    const Group g{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
+    if (p >= 0)
+        process_peak<PACKED>(a, p, P0 + q * a.scratch_stride,
+                             W + q * group_smem_doubles(kSmallG), g);
     __syncwarp();
 }
 
@@ -1065,12 +1014,13 @@ __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
         }
     }
 }
-// Processing order for BATCHED mode: key = (lane-group class << 60) | Morton code of the
-// 0-based (i, j, k), 20 bits per axis; in LEARNED mode the predicted cost (descending)
-// comes before the coarse Morton code.  Peaks consecutive in this order sit close
-// together in the tile, so the warps walking them at the same time gather largely the
-// same cell records, which then come from L2; sorting by class first keeps items of four
-// 8-lane peaks together.  The order changes no result (outputs are indexed by peak).
+// Processing order for BATCHED mode: key = Morton code of the 0-based (i, j, k), 20 bits
+// per axis; in LEARNED mode coarse spatial blocks of 2^block_bits cells (a Morton prefix)
+// and, inside a block, the predicted walk cost (descending).  Peaks consecutive in this
+// order sit close together in the tile, so the warps walking them at the same time
+// gather largely the same cell records, which then come from L2; in LEARNED mode the four
+// peaks of a warp also walk similar distances.  The order changes no result (outputs are
+// indexed by peak).
 __device__ __forceinline__ unsigned long long spread3(unsigned v) {
     unsigned long long x = v & 0xfffffu;
     x = (x | x << 32) & 0x1f00000000ffffULL;
@@ -1093,7 +1043,6 @@ __global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
     if (!keys) return;
     const unsigned i = (unsigned)max(a.pi[p] - 1, 0), j = (unsigned)max(a.pj[p] - 1, 0),
                    k = (unsigned)max(a.pk[p] - 1, 0);
-    const unsigned long long cls = group_size_of(a, b) == kSmallG ? 0ull : 1ull;
     const unsigned long long mort = spread3(i) | (spread3(j) << 1) | (spread3(k) << 2);
     if (cost) {
         // learned order: coarse spatial blocks of 2^block_bits cells (Morton prefix, keeps
@@ -1102,9 +1051,9 @@ __global__ void __launch_bounds__(256) order_key_kernel(const WalkArgs a,
         c = c == c ? fminf(fmaxf(c, 0.f), 1.0e6f) : 0.f;
         const unsigned long long q = min((unsigned long long)(c * 16.f), 0xFFFFFFull);
         const unsigned long long blk = (mort >> a.block_bits) & ((1ull << 38) - 1);
-        keys[p] = (cls << 62) | (blk << 24) | (0xFFFFFFull - q);
+        keys[p] = (blk << 24) | (0xFFFFFFull - q);
     } else {
-        keys[p] = (cls << 60) | mort;
+        keys[p] = mort;
     }
     idx[p] = (int32_t)p;
 }
@@ -1206,7 +1155,6 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.aRnor = 3.0 / alatt;                   // RadialShell.jl:296-300 with hlatt = 1
     a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
     a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
-    a.small_max_shells = ctx->small_max_shells;
     a.block_bits = ctx->tune_block_bits;
     a.queue = nullptr; a.dynamic = 0; a.stats = nullptr;
 }
