@@ -801,8 +801,9 @@ class CpuLeg:
         return {"value": 1.0 / (per_peak_shell + per_peak_find), "unit": UNIT,
                 "cores": self.nthreads, "kind": "port",
                 "sample": f"C restatement of RadialShell.analyse_peak (FP64, {self.nthreads} "
-                          f"threads) on {done} random peaks of the {npk} that find_peaks finds "
-                          f"in the central {SUB}^3 sub-volume (all {len(self.filters)} "
+                          f"threads): {done} analyses of peaks drawn at random from the {npk} "
+                          f"that find_peaks finds in the central {SUB}^3 sub-volume (all "
+                          f"{len(self.filters)} "
                           f"filters, mask carried); find_peaks (1 thread) timed on 130^3 "
                           f"blocks of {len(self.blocks)} filters' fields; per-peak costs of "
                           f"this sample",
