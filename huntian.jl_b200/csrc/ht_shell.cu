@@ -487,7 +487,22 @@ __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck
         // linear offset comes precomputed with its (di, dj, dk)
         const long long cidx = (long long)(ci - 1) + (long long)a.n1 * (cj - 1) +
                                a.s2 * (ck - 1);
-        for (int c = c_begin + g.t; c < c_end; c += g.G) {
+        // two of the lane's cells are requested before either is summed (same summation
+        // order), so their record loads overlap: 473 against 498 ms on the 1152 tile's
+        // walk; four at a time spilled and was no faster
+        int c = c_begin + g.t;
+        for (; c + g.G < c_end; c += 2 * g.G) {
+            const int2 e0 = __ldg(a.cell + c), e1 = __ldg(a.cell + c + g.G);
+            char4 o0, o1;
+            memcpy(&o0, &e0.y, 4);
+            memcpy(&o1, &e1.y, 4);
+            float v0[8], v1[8];
+            CellLoader<PACKED>::load(a, cidx + e0.x, ci + o0.x, cj + o0.y, ck + o0.z, v0);
+            CellLoader<PACKED>::load(a, cidx + e1.x, ci + o1.x, cj + o1.y, ck + o1.z, v1);
+            f(v0, o0);
+            f(v1, o1);
+        }
+        if (c < c_end) {
             const int2 e = __ldg(a.cell + c);
             char4 o;
             memcpy(&o, &e.y, 4);
