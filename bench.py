@@ -389,6 +389,25 @@ class Workload:
         out["speedup_learned_vs_batched"] = w["batched"] / w["learned"]
         return out
 
+    def gather_ceiling(self, n=1 << 26, reps=5):
+        """The rate of scattered 32-byte record gathers with no reuse: uniformly random cells
+        of the packed tile, one 256-bit load each (ht_record_gather_probe), CUDA events,
+        mean of `reps` after a warm-up.  GB/s of gathered records."""
+        ncell = self.nt ** 3
+        g = torch.Generator(device=self.device).manual_seed(7)
+        idx = torch.randint(0, ncell, (n,), device=self.device, generator=g, dtype=torch.int64)
+        out = torch.empty(n, dtype=torch.float32, device=self.device)
+        self.finder.record_gather_probe(idx, out)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            self.finder.record_gather_probe(idx, out)
+        b.record()
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / reps
+        return {"gbs": n * 32 / ms / 1e6, "records": n, "ms": ms}
+
     def release_smoothing(self):
         """Drop the CUDA graph and the smoothing buffers (after the timed steps)."""
         self.graph = None
@@ -506,6 +525,10 @@ def run_ours(args, rank, world, device):
     }
     line["post_step_ms"] = post_step(ht, W)
     line["walk_modes"] = W.walk_modes() if args.compare_modes else None
+    # the walk's second ceiling: scattered 32-byte gathers with no reuse, measured here
+    gc = W.gather_ceiling()
+    line["roofline"]["random_gather_ceiling_gbs"] = gc["gbs"]
+    line["roofline"]["frac_of_random_gather_ceiling"] = achieved / gc["gbs"]
     W.release_smoothing()
     if args.cpu_seconds > 0:
         line["cpu_baseline"], line["parity"] = cpu_baseline(ht, W, args)

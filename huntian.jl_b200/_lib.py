@@ -42,6 +42,7 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_peakfind_filter",
            "ht_fields_pack",
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
+           "ht_record_gather_probe",
            "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
            "ht_bracket_adam", "ht_ctx_tune", "ht_ctx_set_cosmo", "ht_peak_lightcone",
            "ht_pack_halos", "ht_merge_halos", "ht_finalize_eulerian", "ht_evolve_ellipses",
@@ -177,6 +178,8 @@ def load() -> C.CDLL:
                                           dbl, i32, _P, i32, C.POINTER(HtResults), _P]
     L.ht_last_launch_stats.restype = C.c_int
     L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+    L.ht_record_gather_probe.restype = C.c_int
+    L.ht_record_gather_probe.argtypes = [_P, _P, i64, _P, _P]
     L.ht_device_status.restype = C.c_int
     L.ht_device_status.argtypes = [_P, C.POINTER(i32)]
     L.ht_ctx_tune.restype = C.c_int

@@ -1389,3 +1389,55 @@ extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
     ctx->last_kernels = 1;
     return HT_OK;
 }
+
+// ------------------------------------------------------------ measurement aid ----
+//
+// Scattered 32-byte record gathers with the walk's own load, one per index, and nothing
+// else: with random indices this is the gather rate of a walk that found none of its
+// cells in a cache.
+
+namespace {
+
+__global__ void __launch_bounds__(256) record_gather_kernel(const float4* __restrict__ rec,
+                                                            long long ncells,
+                                                            const int64_t* __restrict__ idx,
+                                                            long long n,
+                                                            float* __restrict__ out) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const long long c = __ldg(idx + i);
+        if (c < 0 || c >= ncells) {
+            out[i] = __int_as_float(0x7fc00000);
+            continue;
+        }
+        float v[8];
+        asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+            : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+              "=f"(v[6]), "=f"(v[7])
+            : "l"(rec + 2 * c));
+        out[i] = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+    }
+}
+
+}  // namespace
+
+extern "C" HT_API int ht_record_gather_probe(ht_ctx* ctx, const int64_t* d_idx, int64_t n_idx,
+                                             float* d_out, void* stream) {
+    if (!ctx || (n_idx > 0 && (!d_idx || !d_out)))
+        return ht_fail(HT_ERR_INVALID, "ht_record_gather_probe: NULL argument");
+    if (n_idx < 0) return ht_fail(HT_ERR_INVALID, "ht_record_gather_probe: n_idx < 0");
+    if (!ctx->bound || !ctx->d_rec)
+        return ht_fail(HT_ERR_STATE, "ht_record_gather_probe: no packed tile (ht_fields_pack)");
+    ctx->last_kernels = 0;
+    if (n_idx == 0) return HT_OK;
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    long long blocks = (n_idx + 255) / 256;
+    const long long cap = (long long)ctx->num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    const long long ncells = (long long)ctx->fields.n1 * ctx->fields.n2 * ctx->fields.n3;
+    record_gather_kernel<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(
+        ctx->d_rec, ncells, d_idx, n_idx, d_out);
+    HT_CUDA_TRY(cudaGetLastError(), "record_gather_kernel launch");
+    ctx->last_kernels = 1;
+    return HT_OK;
+}

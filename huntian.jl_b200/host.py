@@ -305,6 +305,18 @@ class HaloFinder:
                                                   _stream_handle(stream)))
         return out
 
+    def record_gather_probe(self, idx: torch.Tensor, out: Optional[torch.Tensor] = None,
+                            stream=None) -> torch.Tensor:
+        """ht_record_gather_probe: the sum of each packed cell record at the 0-based cell
+        indices `idx` (int64, device) of the bound tile, one 256-bit load each -- a
+        measurement of scattered 32-byte gathers (NaN for an index outside the tile)."""
+        assert idx.dtype == torch.int64 and idx.is_contiguous() and idx.is_cuda
+        out = torch.empty(idx.numel(), dtype=torch.float32, device=idx.device) \
+            if out is None else out
+        check(_lib.load().ht_record_gather_probe(self._h, idx.data_ptr(), int(idx.numel()),
+                                                 out.data_ptr(), _stream_handle(stream)))
+        return out
+
     def last_stats(self):
         k, s, c = C.c_int64(), C.c_int64(), C.c_int64()
         check(_lib.load().ht_last_launch_stats(self._h, C.byref(k), C.byref(s), C.byref(c)))

@@ -470,6 +470,16 @@ HT_API int ht_bracket_adam(ht_ctx* ctx, float* d_params, const float* d_grads, f
 HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
                          int64_t* cells_walked);
 
+/* Measurement aid (no reference counterpart): gathers the packed cell records of the bound
+ * tile (ht_fields_pack) at n_idx caller-given cell indices (0-based linear, each < n^3),
+ * with the 256-bit record load the shell walk uses, and writes the sum of each record's
+ * eight values to d_out[i].  With uniformly random indices it measures the rate of
+ * scattered 32-byte gathers without any reuse between them: the memory ceiling of a walk
+ * that found none of its cells in a cache, to set beside the streaming copy bandwidth.
+ * An index outside the tile reads nothing and gives NaN. */
+HT_API int ht_record_gather_probe(ht_ctx* ctx, const int64_t* d_idx, int64_t n_idx,
+                                  float* d_out, void* stream);
+
 /* Device status of the context since the last call (no reference counterpart: the
  * reference kernels have no waits).  Synchronises the device, then returns 0 in *status
  * when every bounded wait of this context's kernels completed, or 1 when a pipeline wait

@@ -219,3 +219,32 @@ def test_large_filter_radius_gradient_window(ht, oracle, julia_table_path):
     for Rf in (1.0, 12.0, 15.0):
         _check(ht, oracle, finder, _fields(d, eta), peaks, 1.0, Rf, 4, 1.0, 1.0, ct, 16,
                "gpu")
+
+
+def test_record_gather_probe(ht, julia_table_path):
+    """ht_record_gather_probe reads the packed record of each given cell (delta, delta at the
+    transposed cell, psi1 xyz, psi2 xyz) with the walk's 256-bit load: its sums equal the
+    same FP32 sums of the fields; an index outside the tile gives NaN."""
+    import torch
+    from gpu_helpers import to_dev
+    rng = np.random.default_rng(5)
+    n = 24
+    f = [rng.standard_normal((n, n, n)).astype(np.float32) for _ in range(7)]
+    tab, axes = ht.read_homeltab(julia_table_path)
+    finder = ht.HaloFinder(4, tab, *axes)
+    finder.bind_fields(*[to_dev(a) for a in f])
+    idx = rng.integers(0, n ** 3, 5000)
+    idx[7] = n ** 3          # outside
+    idx[11] = -1             # outside
+    got = finder.record_gather_probe(torch.as_tensor(idx, dtype=torch.int64, device="cuda"))
+    torch.cuda.synchronize()
+    got = got.cpu().numpy()
+    c = np.clip(idx, 0, n ** 3 - 1)
+    i, j, k = c % n, (c // n) % n, c // (n * n)
+    d = f[0]
+    v = [d[k, j, i], d[j, i, k]] + [a[k, j, i] for a in f[1:]]   # delta[k, i, j] transposed
+    want = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]))
+    ok = (idx >= 0) & (idx < n ** 3)
+    assert np.array_equal(got[ok], want[ok])
+    assert np.isnan(got[~ok]).all()
+    finder.close()
