@@ -477,8 +477,9 @@ struct CellLoader<false> {
 };
 
 // Gather cells [c_begin, c_end) of the r^2-sorted offset list around (ci, cj, ck): lane t
-// of the group takes cells c_begin + t + u G in order and calls f(v, offset) for the
-// in-tile ones.  Out-of-tile cells are skipped (the reference never wraps).
+// of the group takes cells c_begin + t + u G in order and calls f(v, offset, idx, c) for
+// the in-tile ones (idx: the cell's linear index in the tile, c: its place in the list).
+// Out-of-tile cells are skipped (the reference never wraps).
 template <bool PACKED, class F>
 __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck, int c_begin,
                                        int c_end, const Group& g, bool interior, F&& f) {
@@ -499,8 +500,8 @@ __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck
             float v0[8], v1[8];
             CellLoader<PACKED>::load(a, cidx + e0.x, ci + o0.x, cj + o0.y, ck + o0.z, v0);
             CellLoader<PACKED>::load(a, cidx + e1.x, ci + o1.x, cj + o1.y, ck + o1.z, v1);
-            f(v0, o0);
-            f(v1, o1);
+            f(v0, o0, cidx + e0.x, c);
+            f(v1, o1, cidx + e1.x, c + g.G);
         }
         if (c < c_end) {
             const int2 e = __ldg(a.cell + c);
@@ -508,7 +509,7 @@ __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck
             memcpy(&o, &e.y, 4);
             float v[8];
             CellLoader<PACKED>::load(a, cidx + e.x, ci + o.x, cj + o.y, ck + o.z, v);
-            f(v, o);
+            f(v, o, cidx + e.x, c);
         }
         return;
     }
@@ -520,7 +521,7 @@ __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck
                               a.s2 * (iv3 - 1);
         float v[8];
         CellLoader<PACKED>::load(a, idx, iv1, iv2, iv3, v);
-        f(v, o);
+        f(v, o, idx, c);
     }
 }
 
@@ -627,7 +628,7 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         for (int i = 0; i < 13; ++i) acc[i].zero();
         int nin = 0;
         gather<PACKED>(a, ci, cj, ck, st, st + cnt, g, interior,
-                       [&](const float (&v)[8], char4 o) {
+                       [&](const float (&v)[8], char4 o, long long, int) {
             const float d0 = (float)o.x, d1 = (float)o.y, d2 = (float)o.z;
             ++nin;
             acc[0].add(v[0]);
@@ -818,19 +819,36 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
     if (Fbarx * RTHL5 > 0.0) Srb /= (Fbarx * RTHL5);
     g.sync();   // R is reused below
 
+    // cells with r <= RTHL: shells 1..s_in form a contiguous prefix of the cell list
+    const int s_in = last_le(rad, 1, a.nshells, RTHL);
+    const int ncell_in = s_in >= 1 ? __ldg(a.start + s_in) + __ldg(a.count + s_in) : 0;
+
     // Sbar, Sbar2 (RadialShell.jl:739-754): mean psi over the in-tile cells of shells
-    // 1..m0f-1, a contiguous prefix of the cell list
+    // 1..m0f-1; and the mask: the core cells within RTHL (ShellAnalysisGPU.jl:513-528,
+    // RadialShell.jl:773-782).  Both are prefixes of the cell list that differ by at most
+    // shell m0f (RTHL lies between rad[m0f - 1] and rad[m0f]), so one pass over the longer
+    // prefix serves both (a separate mask pass cost 3 % of the walk on the 1152 tile).
     double Sb[3], Sb2[3];
     {
         const int ncell = __ldg(a.start + m0f);
+        const int nmask = a.mask ? ncell_in : 0;
         Acc ks[6];
 #pragma unroll
         for (int i = 0; i < 6; ++i) ks[i].zero();
         int nloc = 0;
-        gather<PACKED>(a, ci, cj, ck, 0, ncell, g, interior, [&](const float (&v)[8], char4) {
+        gather<PACKED>(a, ci, cj, ck, 0, max(ncell, nmask), g, interior,
+                       [&](const float (&v)[8], char4 o, long long idx, int c) {
+            if (c < ncell) {
 #pragma unroll
-            for (int i = 0; i < 6; ++i) ks[i].add(v[2 + i]);
-            ++nloc;
+                for (int i = 0; i < 6; ++i) ks[i].add(v[2 + i]);
+                ++nloc;
+            }
+            if (c < nmask) {
+                const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
+                if (iv1 > a.nbuff && iv1 <= a.n1 - a.nbuff && iv2 > a.nbuff &&
+                    iv2 <= a.n2 - a.nbuff && iv3 > a.nbuff && iv3 <= a.n3 - a.nbuff)
+                    a.mask[idx] = 1;
+            }
         });
         const double nS = g.sum((double)nloc);
 #pragma unroll
@@ -840,10 +858,6 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
             Sb2[L] = nS > 0.0 ? s2v / nS : 0.0;
         }
     }
-
-    // cells with r <= RTHL: shells 1..s_in form a contiguous prefix of the cell list
-    const int s_in = last_le(rad, 1, a.nshells, RTHL);
-    const int ncell_in = s_in >= 1 ? __ldg(a.start + s_in) + __ldg(a.count + s_in) : 0;
 
     // d2F
     double d2F = 0.0;
@@ -888,20 +902,6 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         const double tot = g.sum(ks.value());
         const double nt = g.sum((double)nloc);
         if (nt > 0.0) d2F = tot / nt;
-    }
-
-    // mask: core cells within RTHL (ShellAnalysisGPU.jl:513-528, RadialShell.jl:773-782)
-    if (a.mask) {
-        for (int c = t; c < ncell_in; c += G) {
-            const char4 o = __ldg(a.off + c);
-            const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
-            if (iv1 > a.nbuff && iv1 <= a.n1 - a.nbuff && iv2 > a.nbuff &&
-                iv2 <= a.n2 - a.nbuff && iv3 > a.nbuff && iv3 <= a.n3 - a.nbuff) {
-                const long long idx = (long long)(iv1 - 1) + (long long)a.n1 * (iv2 - 1) +
-                                      a.s2 * (iv3 - 1);
-                a.mask[idx] = 1;
-            }
-        }
     }
 
     // zvir_half (RadialShell.jl:801-859): radius jj is handled by lane (jj - 1) % G
