@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libhuntian_b200.so")
+# HT_CHECKED=1 selects the bounds-checked build (build.py --checked), same C ABI
+LIB_PATH = os.path.join(_HERE, "libhuntian_b200_checked.so" if os.environ.get("HT_CHECKED") == "1"
+                        else "libhuntian_b200.so")
 
 HT_OK = 0
 HT_ERR_INVALID = 1
@@ -32,6 +34,8 @@ HT_TUNE_WALK_BPSM = 3
 HT_TUNE_FFT_PATH = 4
 HT_TUNE_WAIT_NS = 5
 HT_TUNE_INJECT_TX = 6
+# reject reasons (HT_REJECT_*), in counter order
+REJECT_REASONS = ("premask", "no_fcrit", "m0_one", "no_collapse", "rthl_neg", "outside")
 
 # every symbol include/huntian_b200.h declares
 SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_info",
@@ -42,6 +46,7 @@ SYMBOLS = ("ht_ctx_create", "ht_ctx_destroy", "ht_last_error", "ht_ctx_shell_inf
            "ht_peakfind_filter",
            "ht_fields_pack",
            "ht_shell_analyse", "ht_shell_analyse_static", "ht_last_launch_stats",
+           "ht_reject_counts", "ht_reset_reject_counts",
            "ht_record_gather_probe",
            "ht_device_status", "ht_bracket_features", "ht_bracket_predict", "ht_bracket_grad",
            "ht_bracket_adam", "ht_ctx_tune", "ht_ctx_set_cosmo", "ht_peak_lightcone",
@@ -178,6 +183,10 @@ def load() -> C.CDLL:
                                           dbl, i32, _P, i32, C.POINTER(HtResults), _P]
     L.ht_last_launch_stats.restype = C.c_int
     L.ht_last_launch_stats.argtypes = [_P, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64)]
+    L.ht_reject_counts.restype = C.c_int
+    L.ht_reject_counts.argtypes = [_P, C.POINTER(i64)]
+    L.ht_reset_reject_counts.restype = C.c_int
+    L.ht_reset_reject_counts.argtypes = [_P, _P]
     L.ht_record_gather_probe.restype = C.c_int
     L.ht_record_gather_probe.argtypes = [_P, _P, i64, _P, _P]
     L.ht_device_status.restype = C.c_int

@@ -242,6 +242,7 @@ static int upload(T** dst, const T* src, size_t n, const char* what) {
 extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, int nx, int ny,
                              int nz, double X1, double X2, double Y1, double Y2, double Z1,
                              double Z2, double out_val, ht_ctx** out) {
+    HT_RANGE("ht_ctx_create");
     if (!out) return ht_fail(HT_ERR_INVALID, "ht_ctx_create: out is NULL");
     *out = nullptr;
     if (nhunt < 1 || nhunt > 127)
@@ -297,6 +298,7 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
 }
 
 extern "C" int ht_ctx_destroy(ht_ctx* ctx) {
+    HT_RANGE("ht_ctx_destroy");
     if (!ctx) return HT_OK;
     cudaSetDevice(ctx->device);
     free_ctx(ctx);
@@ -332,6 +334,7 @@ extern "C" int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const flo
                                   int8_t* d_mask, int n, int nbuff, float fcrit,
                                   int32_t filter_idx, int64_t max_peaks, const ht_peaks* out,
                                   void* stream) {
+    HT_RANGE("ht_peakfind_filter");
     if (!ctx || !d_delta_s || !d_mask || !out)
         return ht_fail(HT_ERR_INVALID, "ht_peakfind_filter: NULL argument");
     if (!out->i || !out->j || !out->k || !out->delta || !out->filter_idx || !out->count)
@@ -349,6 +352,7 @@ extern "C" int ht_peakfind_filter(ht_ctx* ctx, const float* d_delta_s, const flo
 }
 
 extern "C" int ht_fields_pack(ht_ctx* ctx, const ht_fields* f, void* stream) {
+    HT_RANGE("ht_fields_pack");
     if (!ctx || !f) return ht_fail(HT_ERR_INVALID, "ht_fields_pack: NULL argument");
     if (!f->delta || !f->etax || !f->etay || !f->etaz)
         return ht_fail(HT_ERR_INVALID, "ht_fields_pack: delta and eta x/y/z are required");
@@ -375,6 +379,7 @@ extern "C" int ht_fields_pack(ht_ctx* ctx, const ht_fields* f, void* stream) {
 extern "C" int ht_shell_analyse(ht_ctx* ctx, const ht_peak_batch* b, double alatt,
                                 double rmax2rs, int32_t nbuff, int8_t* d_mask, int32_t conv,
                                 int32_t mode, const ht_results* out, void* stream) {
+    HT_RANGE("ht_shell_analyse");
     if (!ctx || !b || !out) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: NULL argument");
     if (!ctx->bound) return ht_fail(HT_ERR_STATE, "ht_shell_analyse: call ht_fields_pack first");
     if (b->npeaks < 0) return ht_fail(HT_ERR_INVALID, "ht_shell_analyse: npeaks < 0");
@@ -418,7 +423,31 @@ extern "C" int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t
     return HT_OK;
 }
 
+extern "C" int ht_reject_counts(const ht_ctx* ctx, int64_t* counts) {
+    HT_RANGE("ht_reject_counts");
+    if (!ctx || !counts) return ht_fail(HT_ERR_INVALID, "ht_reject_counts: NULL argument");
+    unsigned long long h[HT_REJECT_COUNT];
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    HT_CUDA_TRY(cudaDeviceSynchronize(), "ht_reject_counts: synchronize");
+    HT_CUDA_TRY(cudaMemcpy(h, ctx->d_stats + 16, sizeof h, cudaMemcpyDeviceToHost),
+                "reject counters read");
+    for (int i = 0; i < HT_REJECT_COUNT; ++i) counts[i] = (int64_t)h[i];
+    return HT_OK;
+}
+
+extern "C" int ht_reset_reject_counts(ht_ctx* ctx, void* stream) {
+    HT_RANGE("ht_reset_reject_counts");
+    if (!ctx) return ht_fail(HT_ERR_INVALID, "ht_reset_reject_counts: ctx is NULL");
+    HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    HT_CUDA_TRY(cudaMemsetAsync(ht_reject_words(ctx), 0,
+                                HT_REJECT_COUNT * sizeof(unsigned long long),
+                                (cudaStream_t)stream),
+                "reject counters reset");
+    return HT_OK;
+}
+
 extern "C" int ht_device_status(ht_ctx* ctx, int32_t* status) {
+    HT_RANGE("ht_device_status");
     if (!ctx || !status) return ht_fail(HT_ERR_INVALID, "ht_device_status: NULL argument");
     HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
     HT_CUDA_TRY(cudaDeviceSynchronize(), "ht_device_status: synchronize");

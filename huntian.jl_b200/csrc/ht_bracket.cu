@@ -420,6 +420,7 @@ unsigned blocks_for(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 extern "C" HT_API int ht_bracket_features(ht_ctx* ctx, const ht_peak_batch* b,
                                           const float* d_peak_delta, double alatt,
                                           float* d_feat, void* stream) {
+    HT_RANGE("ht_bracket_features");
     if (!ctx || !b || !d_feat) return ht_fail(HT_ERR_INVALID, "ht_bracket_features: NULL argument");
     if (!ctx->bound) return ht_fail(HT_ERR_STATE, "ht_bracket_features: no tile bound (ht_fields_pack)");
     if (b->npeaks < 0) return ht_fail(HT_ERR_INVALID, "ht_bracket_features: npeaks < 0");
@@ -446,6 +447,7 @@ extern "C" HT_API int ht_bracket_features(ht_ctx* ctx, const ht_peak_batch* b,
 extern "C" HT_API int ht_bracket_predict(ht_ctx* ctx, const ht_bracket_model* m,
                                          const float* d_feat, int64_t n, float* d_pred,
                                          void* stream) {
+    HT_RANGE("ht_bracket_predict");
     if (!ctx || !d_feat || !d_pred) return ht_fail(HT_ERR_INVALID, "ht_bracket_predict: NULL argument");
     int rc = check_model(m, "ht_bracket_predict");
     if (rc != HT_OK) return rc;
@@ -463,6 +465,7 @@ extern "C" HT_API int ht_bracket_predict(ht_ctx* ctx, const ht_bracket_model* m,
 extern "C" HT_API int ht_bracket_grad(ht_ctx* ctx, const ht_bracket_model* m,
                                       const float* d_feat, const float* d_target, int64_t n,
                                       float* d_grads, float* d_loss, void* stream) {
+    HT_RANGE("ht_bracket_grad");
     if (!ctx || !d_feat || !d_target || !d_grads || !d_loss)
         return ht_fail(HT_ERR_INVALID, "ht_bracket_grad: NULL argument");
     int rc = check_model(m, "ht_bracket_grad");
@@ -538,6 +541,7 @@ extern "C" HT_API int ht_bracket_grad(ht_ctx* ctx, const ht_bracket_model* m,
 extern "C" HT_API int ht_bracket_adam(ht_ctx* ctx, float* d_params, const float* d_grads,
                                       float* d_m, float* d_v, int32_t step, float lr,
                                       const ht_bracket_model* out, void* stream) {
+    HT_RANGE("ht_bracket_adam");
     if (!ctx || !d_params || !d_grads || !d_m || !d_v)
         return ht_fail(HT_ERR_INVALID, "ht_bracket_adam: NULL argument");
     int rc = check_model(out, "ht_bracket_adam");

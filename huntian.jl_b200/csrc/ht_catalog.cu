@@ -280,6 +280,7 @@ int catalog_workspace(ht_ctx* ctx, long long npeaks, uint8_t** flags, int32_t** 
 }  // namespace
 
 extern "C" HT_API int ht_ctx_set_cosmo(ht_ctx* ctx, const ht_cosmo* c) {
+    HT_RANGE("ht_ctx_set_cosmo");
     if (!ctx || !c) return ht_fail(HT_ERR_INVALID, "ht_ctx_set_cosmo: NULL argument");
     if (!c->chi || !c->zchi || c->n_chi < 2 || !c->atab || !c->D_atab || !c->dlnD_dlna ||
         c->ntab < 4)
@@ -323,6 +324,7 @@ extern "C" HT_API int ht_peak_lightcone(ht_ctx* ctx, const int32_t* d_i, const i
                                         double z_max, double* d_z, float* d_ZZon,
                                         float* d_fcrit, int32_t* d_keep, int64_t* d_nkeep,
                                         void* stream) {
+    HT_RANGE("ht_peak_lightcone");
     if (!ctx || !geom || !obs || !d_ZZon || !d_fcrit || !d_keep || !d_nkeep ||
         (npeaks > 0 && (!d_i || !d_j || !d_k)))
         return ht_fail(HT_ERR_INVALID, "ht_peak_lightcone: NULL argument");
@@ -365,6 +367,7 @@ extern "C" HT_API int ht_pack_halos(ht_ctx* ctx, const ht_catalog_peaks* peaks,
                                     double ZZon, double z_max, int32_t ilpt,
                                     int32_t ioutshear, float* d_records, int64_t cap,
                                     int64_t* d_nhalo, void* stream) {
+    HT_RANGE("ht_pack_halos");
     if (!ctx || !peaks || !res || !geom || !d_nhalo || (cap > 0 && !d_records))
         return ht_fail(HT_ERR_INVALID, "ht_pack_halos: NULL argument");
     if (!ctx->cosmo_set) return ht_fail(HT_ERR_STATE, "ht_pack_halos: call ht_ctx_set_cosmo first");

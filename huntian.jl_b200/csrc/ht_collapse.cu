@@ -442,6 +442,7 @@ extern "C" HT_API int ht_evolve_ellipses(int device, const ht_ellipsoid* ep,
                                          const double* d_p_v, int32_t idynax, double* d_zvir,
                                          double* d_D, double* d_fc, int32_t* d_steps,
                                          void* stream) {
+    HT_RANGE("ht_evolve_ellipses");
     int rc = check_inputs(ep, growth, "ht_evolve_ellipses");
     if (rc != HT_OK) return rc;
     if (n < 0) return ht_fail(HT_ERR_INVALID, "ht_evolve_ellipses: n < 0");
@@ -481,6 +482,7 @@ extern "C" HT_API int ht_collapse_table(int device, const ht_ellipsoid* ep,
                                         const ht_growth* growth, int32_t nx, int32_t ny,
                                         int32_t nz, double X1, double X2, double Y1, double Y2,
                                         double Z1, double Z2, float* table) {
+    HT_RANGE("ht_collapse_table");
     int rc = check_inputs(ep, growth, "ht_collapse_table");
     if (rc != HT_OK) return rc;
     if (nx < 2 || ny < 2 || nz < 2)

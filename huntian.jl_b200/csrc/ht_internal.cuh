@@ -1,6 +1,9 @@
 // Internal declarations shared by the huntian_b200 CUDA sources.
 #pragma once
 
+#ifndef HT_NO_NVTX
+#include <nvtx3/nvToolsExt.h>
+#endif
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <stdint.h>
@@ -112,7 +115,8 @@ struct ht_ctx {
     size_t merge_scan_bytes = 0;
     int32_t* d_queue = nullptr;    // dynamic work counter
     unsigned long long* d_stats = nullptr;  // [0] cells walked, [1] shells walked,
-                                            // [8] (int32) device status word
+                                            // [8] (int32) device status word,
+                                            // [16, 16 + HT_REJECT_COUNT) reject counters
 
     int64_t last_kernels = 0;
 };
@@ -120,6 +124,43 @@ struct ht_ctx {
 // Device status word: kernels with bounded waits store a non-zero code here when a wait
 // gives up, instead of trapping; ht_device_status reads and clears it.
 inline int32_t* ht_status_word(ht_ctx* ctx) { return (int32_t*)(ctx->d_stats + 8); }
+
+// Status codes in the device status word (ht_device_status).
+constexpr int32_t kStatusWaitTimeout = 1;   // a bounded wait gave up
+constexpr int32_t kStatusBounds = 2;        // an HT_CHECKED index check failed
+
+// HT_CHECKED builds: an index check before a data-dependent access.  A failed check
+// records kStatusBounds in the status word and evaluates to false, so that the caller
+// skips the access (no trap); other builds compile the check away.
+#ifdef HT_CHECKED
+__device__ __forceinline__ bool ht_index_ok(int32_t* status, long long i, long long n) {
+    if (i >= 0 && i < n) return true;
+    if (status) atomicExch(status, kStatusBounds);
+    return false;
+}
+#define HT_INDEX_OK(status, i, n) ht_index_ok((status), (long long)(i), (long long)(n))
+#else
+#define HT_INDEX_OK(status, i, n) true
+#endif
+
+// Reject-reason counters (HT_REJECT_*), accumulated by the shell walk until reset.
+inline unsigned long long* ht_reject_words(ht_ctx* ctx) { return ctx->d_stats + 16; }
+
+// NVTX range around a C-ABI entry point: each call shows as a named range on the host
+// timeline of a profiler that records NVTX (Nsight Systems; Nsight Compute with --nvtx).
+// nvtx3 is header-only and its calls do nothing unless a profiler has attached.  Built
+// with -DHT_NO_NVTX the ranges compile away.
+#ifndef HT_NO_NVTX
+struct HtRange {
+    explicit HtRange(const char* name) { nvtxRangePushA(name); }
+    ~HtRange() { nvtxRangePop(); }
+    HtRange(const HtRange&) = delete;
+    HtRange& operator=(const HtRange&) = delete;
+};
+#define HT_RANGE(name) HtRange ht_nvtx_range_(name)
+#else
+#define HT_RANGE(name) ((void)0)
+#endif
 
 // ----------------------------------------------------------------- errors ----
 

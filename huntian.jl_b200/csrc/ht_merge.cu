@@ -346,6 +346,7 @@ extern "C" HT_API int ht_merge_halos(ht_ctx* ctx, const float* d_records, int64_
                                      int32_t width, int32_t volume_reduction,
                                      int32_t fortran_ties, float* d_out, int64_t* d_nout,
                                      void* stream) {
+    HT_RANGE("ht_merge_halos");
     if (!ctx || !d_nout || (nhalo > 0 && (!d_records || !d_out)))
         return ht_fail(HT_ERR_INVALID, "ht_merge_halos: NULL argument");
     if (width != 11 && width != 33)
@@ -529,6 +530,7 @@ extern "C" HT_API int ht_merge_halos(ht_ctx* ctx, const float* d_records, int64_
 extern "C" HT_API int ht_finalize_eulerian(ht_ctx* ctx, float* d_records, int64_t nhalo,
                                            int32_t width, const double* obs, int32_t ievol,
                                            double z_out, void* stream) {
+    HT_RANGE("ht_finalize_eulerian");
     if (!ctx || (nhalo > 0 && !d_records) || (ievol == 1 && !obs))
         return ht_fail(HT_ERR_INVALID, "ht_finalize_eulerian: NULL argument");
     if (width != 11 && width != 33)

@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(kTX * kTY) pf_flag_tma_kernel(
     }
     if (!ok && tid == 0) {
         // record the timeout, then wait (bounded) for the copies still in flight
-        atomicExch(status, 1);
+        atomicExch(status, kStatusWaitTimeout);
         for (int q = s_now; q < issued; ++q)
             bar_wait(&full[q % kStages], (unsigned)((q / kStages) & 1), wait_ns);
     }
@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(1024) pf_scan_kernel(const int32_t* __restrict
 __global__ void __launch_bounds__(kEmitThreads) pf_emit_kernel(
     const uint32_t* __restrict__ bits, PfGeom g, const int64_t* __restrict__ segbase,
     const float* __restrict__ ds, const float* __restrict__ lapd_s, int8_t* __restrict__ mask,
-    int32_t filter_idx, int64_t max_peaks, ht_peaks out) {
+    int32_t filter_idx, int64_t max_peaks, ht_peaks out, int32_t* status) {
     __shared__ int warp_tot[kEmitThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const long long w0 = (long long)blockIdx.x * kSegWords + (long long)tid * kWordsPerThread;
@@ -390,6 +390,7 @@ __global__ void __launch_bounds__(kEmitThreads) pf_emit_kernel(
             if (slot >= max_peaks) return;
             const int i = g.nbuff + ib + b, j = g.nbuff + jj, k = g.nbuff + kk;   // 0-based
             const long long cidx = (long long)i + n * j + nn * k;
+            if (!HT_INDEX_OK(status, cidx, nn * n)) continue;
             out.i[slot] = i + 1;
             out.j[slot] = j + 1;
             out.k[slot] = k + 1;
@@ -483,7 +484,8 @@ int ht_launch_peakfind(ht_ctx* ctx, const float* d_delta_s, const float* d_lapd_
     HT_CUDA_TRY(cudaGetLastError(), "pf_scan_kernel launch");
     pf_emit_kernel<<<(unsigned)nseg, kEmitThreads, 0, st>>>(bits, g, segbase, d_delta_s,
                                                              d_lapd_s, d_mask, filter_idx,
-                                                             max_peaks, *out);
+                                                             max_peaks, *out,
+                                                             ht_status_word(ctx));
     HT_CUDA_TRY(cudaGetLastError(), "pf_emit_kernel launch");
     ctx->last_kernels = 4;
     return HT_OK;

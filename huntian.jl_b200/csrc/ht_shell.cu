@@ -115,6 +115,10 @@ struct WalkArgs {
     int32_t* queue;
     int dynamic;
     unsigned long long* stats;
+    unsigned long long* reject;   // nullable: the context's HT_REJECT_* counters
+    int32_t* status;              // the context's status word (HT_CHECKED index checks)
+    long long ntile;              // n1 n2 n3: cells of the bound tile
+    long long ncells;             // entries of the offset and cell tables
 };
 
 // ------------------------------------------------------------ small helpers ----
@@ -449,6 +453,10 @@ struct CellLoader<true> {
     // L1 request per cell instead of two
     __device__ __forceinline__ static void load(const WalkArgs& a, long long idx, int, int,
                                                 int, float (&v)[8]) {
+        if (!HT_INDEX_OK(a.status, idx, a.ntile)) {
+            for (int i = 0; i < 8; ++i) v[i] = __int_as_float(0x7fc00000);
+            return;
+        }
         asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
             : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
               "=f"(v[6]), "=f"(v[7])
@@ -463,6 +471,10 @@ struct CellLoader<false> {
         // transposed read delta[iv3, iv1, iv2] (ext/CUDAExt.jl:819-820), cubic tile
         const long long idt = (long long)(iv3 - 1) + (long long)a.n1 * (iv1 - 1) +
                               a.s2 * (iv2 - 1);
+        if (!HT_INDEX_OK(a.status, idx, a.ntile) || !HT_INDEX_OK(a.status, idt, a.ntile)) {
+            for (int i = 0; i < 8; ++i) v[i] = __int_as_float(0x7fc00000);
+            return;
+        }
         v[0] = __ldg(a.delta + idx);
         v[1] = __ldg(a.delta + idt);
         v[2] = __ldg(a.ex + idx);
@@ -483,6 +495,7 @@ struct CellLoader<false> {
 template <bool PACKED, class F>
 __device__ __forceinline__ void gather(const WalkArgs& a, int ci, int cj, int ck, int c_begin,
                                        int c_end, const Group& g, bool interior, F&& f) {
+    if (c_end > c_begin && !HT_INDEX_OK(a.status, c_end - 1, a.ncells)) return;
     if (interior) {
         // every offset of the table stays inside the tile: no bounds test, and the cell's
         // linear offset comes precomputed with its (di, dj, dk)
@@ -587,9 +600,14 @@ __device__ __forceinline__ Bounds bounds_of(const WalkArgs& a, long long p) {
     return peak_bounds(a, a.Rf[p], a.ir2min[p]);
 }
 
+// One count of reject reason r in the block's shared counters (lane 0 of the group).
+__device__ __forceinline__ void count_reject(unsigned* rej, const Group& g, int r) {
+    if (g.t == 0) atomicAdd(rej + r, 1u);
+}
+
 template <bool PACKED>
 __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, double* __restrict__ P,
-                             double* __restrict__ R, const Group& g) {
+                             double* __restrict__ R, const Group& g, unsigned* rej) {
     const double* rad = a.rad;
     const int G = g.G, t = g.t, RP = G + 1;
     const int ci = a.pi[p], cj = a.pj[p], ck = a.pk[p];
@@ -599,11 +617,17 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         // a centre outside the tile has no cells to walk (the reference would fault)
         write_walk_shells(a, p, g, 0);
         write_no_collapse(a, p, g);
+        count_reject(rej, g, HT_REJECT_OUTSIDE);
         return;
     }
     const Bounds bd = bounds_of(a, p);
     const int m = bd.m;
-    if (m < 2) { write_walk_shells(a, p, g, 1); write_no_collapse(a, p, g); return; }
+    if (m < 2) {
+        write_walk_shells(a, p, g, 1);
+        write_no_collapse(a, p, g);
+        count_reject(rej, g, HT_REJECT_NO_COLLAPSE);
+        return;
+    }
 
     // ---------------------------------------------------------------- walk ----
     float cv[8];
@@ -666,6 +690,7 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         const double r5 = rs * rs * rs * rs * rs;
         csrb += 0.5 * (Fbarp + Fbar_s) * (r5 - rad5p);
         double* q = P + (size_t)s * kRec;
+        if (!HT_INDEX_OK(a.status, s, a.nshells + 2)) break;
         for (int i = t; i <= P_CSRB; i += G) {
             double v;
             if (i == P_FBAR) v = Fbar_s;
@@ -719,7 +744,11 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
                 found = true;
             }
         }
-        if (!found) { write_no_collapse(a, p, g); return; }
+        if (!found) {   // RadialShell.jl:516-518
+            write_no_collapse(a, p, g);
+            count_reject(rej, g, HT_REJECT_NO_FCRIT);
+            return;
+        }
     }
 
     // inward walk (RadialShell.jl:529-686): step u evaluates shell m0 - u; step 0 is m0
@@ -753,7 +782,14 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         for (int i = t; i < 14; i += G) R[G * kStepW + i] = R[(G - 1) * kStepW + i];
         g.sync();
     }
-    if (tstar < 0 || (tstar == 0 && m0 == 1)) { write_no_collapse(a, p, g); return; }
+    if (tstar < 0 || (tstar == 0 && m0 == 1)) {
+        // m0 = 1 without a collapse at the centre: RadialShell.jl:603-605; no collapse:
+        // :683-685; a collapse at the centre shell has no inner radius (RTHL <= 0)
+        write_no_collapse(a, p, g);
+        count_reject(rej, g, tstar == 0 ? HT_REJECT_RTHL_NEG
+                             : m0 == 1 ? HT_REJECT_M0_ONE : HT_REJECT_NO_COLLAPSE);
+        return;
+    }
     if (tstar == 0) prow = lrow;
     const double* Lr = R + lrow * kStepW;   // collapse step ("last")
     const double* Pr = R + prow * kStepW;   // the step before it ("prev")
@@ -770,7 +806,11 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
     } else {
         RTHL = rp;
     }
-    if (RTHL <= 0.0) { write_no_collapse(a, p, g); return; }
+    if (RTHL <= 0.0) {   // RadialShell.jl:697-699
+        write_no_collapse(a, p, g);
+        count_reject(rej, g, HT_REJECT_RTHL_NEG);
+        return;
+    }
 
     const double RTHL3 = RTHL * RTHL * RTHL, RTHL5 = RTHL3 * RTHL * RTHL;
     const double rad3p = rp * rp * rp, rad3 = rm * rm * rm, drad3 = rad3 - rad3p;
@@ -846,7 +886,8 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
             if (c < nmask) {
                 const int iv1 = ci + o.x, iv2 = cj + o.y, iv3 = ck + o.z;
                 if (iv1 > a.nbuff && iv1 <= a.n1 - a.nbuff && iv2 > a.nbuff &&
-                    iv2 <= a.n2 - a.nbuff && iv3 > a.nbuff && iv3 <= a.n3 - a.nbuff)
+                    iv2 <= a.n2 - a.nbuff && iv3 > a.nbuff && iv3 <= a.n3 - a.nbuff &&
+                    HT_INDEX_OK(a.status, idx, a.ntile))
                     a.mask[idx] = 1;
             }
         });
@@ -985,7 +1026,7 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
 // group of kSmallG lanes; group q of warp w owns scratch slot kPeaksPerItem w + q.
 template <bool PACKED>
 __device__ __forceinline__ void process_item(const WalkArgs& a, long long item, double* P0,
-                                             double* W, int lane) {
+                                             double* W, int lane, unsigned* rej) {
     const int q = lane / kSmallG;
     const long long e = item * kPeaksPerItem + q;
     long long p = -1;
@@ -996,7 +1037,7 @@ __device__ __forceinline__ void process_item(const WalkArgs& a, long long item, 
     const Group g{kSmallG, lane % kSmallG, q, ((1u << kSmallG) - 1u) << (q * kSmallG)};
     if (p >= 0)
         process_peak<PACKED>(a, p, P0 + q * a.scratch_stride,
-                             W + q * group_smem_doubles(kSmallG), g);
+                             W + q * group_smem_doubles(kSmallG), g, rej);
     __syncwarp();
 }
 
@@ -1004,6 +1045,9 @@ __device__ __forceinline__ void process_item(const WalkArgs& a, long long item, 
 template <bool PACKED>
 __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
     extern __shared__ double smem[];
+    __shared__ unsigned rej[HT_REJECT_COUNT];   // the block's reject counts
+    if (threadIdx.x < HT_REJECT_COUNT) rej[threadIdx.x] = 0u;
+    __syncthreads();
     const int lane = threadIdx.x & 31;
     double* W = smem + (threadIdx.x >> 5) * kWarpSmemDoubles;
     const long long gw = (long long)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
@@ -1019,7 +1063,7 @@ __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
         item = gw;
     }
     while (item < nitems) {
-        process_item<PACKED>(a, item, P0, W, lane);
+        process_item<PACKED>(a, item, P0, W, lane, rej);
         if (a.dynamic) {
             int q = 0;
             if (lane == 0) q = atomicAdd(a.queue, 1);
@@ -1028,6 +1072,9 @@ __global__ void __launch_bounds__(kThreads, 3) walk_kernel(const WalkArgs a) {
             item += nw;
         }
     }
+    __syncthreads();
+    if (threadIdx.x < HT_REJECT_COUNT && a.reject && rej[threadIdx.x])
+        atomicAdd(a.reject + threadIdx.x, (unsigned long long)rej[threadIdx.x]);
 }
 // Processing order for BATCHED mode: key = Morton code of the 0-based (i, j, k), 20 bits
 // per axis; in LEARNED mode coarse spatial blocks of 2^block_bits cells (a Morton prefix)
@@ -1171,7 +1218,9 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.wRnor = 3.0 * (1.0 / (4.0 * pi)) / alatt;
     a.rmax2rs = rmax2rs; a.nbuff = nbuff; a.conv = conv; a.mask = d_mask; a.out = *out;
     a.block_bits = ctx->tune_block_bits;
-    a.queue = nullptr; a.dynamic = 0; a.stats = nullptr;
+    a.queue = nullptr; a.dynamic = 0; a.stats = nullptr; a.reject = ctx->d_stats + 16;
+    a.status = (int32_t*)(ctx->d_stats + 8);
+    a.ntile = (long long)f.n1 * f.n2 * f.n3; a.ncells = ctx->ncells;
 }
 
 static size_t walk_smem_bytes() {
@@ -1328,6 +1377,7 @@ extern "C" HT_API int ht_shell_analyse_static(ht_ctx* ctx, const ht_fields* f,
                                               double rmax2rs, int32_t nbuff, int8_t* d_mask,
                                               int32_t conv, const ht_results* out,
                                               void* stream) {
+    HT_RANGE("ht_shell_analyse_static");
     if (!ctx || !f || !b || !out)
         return ht_fail(HT_ERR_INVALID, "ht_shell_analyse_static: NULL argument");
     if (!f->delta || !f->etax || !f->etay || !f->etaz)
@@ -1423,6 +1473,7 @@ __global__ void __launch_bounds__(256) record_gather_kernel(const float4* __rest
 
 extern "C" HT_API int ht_record_gather_probe(ht_ctx* ctx, const int64_t* d_idx, int64_t n_idx,
                                              float* d_out, void* stream) {
+    HT_RANGE("ht_record_gather_probe");
     if (!ctx || (n_idx > 0 && (!d_idx || !d_out)))
         return ht_fail(HT_ERR_INVALID, "ht_record_gather_probe: NULL argument");
     if (n_idx < 0) return ht_fail(HT_ERR_INVALID, "ht_record_gather_probe: n_idx < 0");

@@ -95,6 +95,7 @@ int check_window_args(const char* who, double boxsize, double Rf) {
 
 extern "C" HT_API int ht_smooth_window(ht_ctx* ctx, const void* d_delta_k, void* d_out, int n,
                                        double boxsize, double Rf, int wsmooth, void* stream) {
+    HT_RANGE("ht_smooth_window");
     if (!ctx || !d_delta_k || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: NULL argument");
     if (n < 2 || n > 8192) return ht_fail(HT_ERR_INVALID, "ht_smooth_window: need 2 <= n <= 8192");
     int rc = check_window_args("ht_smooth_window", boxsize, Rf);
@@ -745,7 +746,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     }
     if (!ok && tid == 0) {
         // record the timeout, then wait (bounded) for the copy still in flight
-        atomicExch(status, 1);
+        atomicExch(status, kStatusWaitTimeout);
         htasync::bar_wait(&bar, parity, wait_ns);
     }
 }
@@ -817,7 +818,7 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
         }
     }
     if (!ok && tid == 0) {
-        atomicExch(status, 1);
+        atomicExch(status, kStatusWaitTimeout);
         htasync::bar_wait(&bar, parity, wait_ns);
     }
 }
@@ -901,7 +902,7 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
     }
     if (!ok && lane == 0) {
         // record the timeout, then wait (bounded) for this warp's copies in flight
-        atomicExch(status, 1);
+        atomicExch(status, kStatusWaitTimeout);
         htasync::bar_wait(&bar[i & 1], (unsigned)((i >> 1) & 1), wait_ns);
         if (r + stride < rows)
             htasync::bar_wait(&bar[(i & 1) ^ 1], (unsigned)(((i + 1) >> 1) & 1), wait_ns);
@@ -1031,6 +1032,7 @@ extern "C" HT_API int ht_smooth_pencil_supported(int n) { return pencil_side(n) 
 
 extern "C" HT_API int ht_spectrum_pencil(ht_ctx* ctx, const void* d_delta_k, void* d_pencil,
                                          int n, void* stream) {
+    HT_RANGE("ht_spectrum_pencil");
     if (!ctx || !d_delta_k || !d_pencil) return ht_fail(HT_ERR_INVALID, "ht_spectrum_pencil: NULL argument");
     if (n < 2 || n > 4096 || (n & 1))
         return ht_fail(HT_ERR_INVALID, "ht_spectrum_pencil: need an even n, 2 <= n <= 4096");
@@ -1048,6 +1050,7 @@ extern "C" HT_API int ht_spectrum_pencil(ht_ctx* ctx, const void* d_delta_k, voi
 extern "C" HT_API int ht_smooth_pencil(ht_ctx* ctx, const void* d_pencil, float* d_out, int n,
                                        double boxsize, double Rf, int wsmooth, int lo, int hi,
                                        void* stream) {
+    HT_RANGE("ht_smooth_pencil");
     if (!ctx || !d_pencil || !d_out) return ht_fail(HT_ERR_INVALID, "ht_smooth_pencil: NULL argument");
     if (!pencil_side(n))
         return ht_fail(HT_ERR_INVALID, "ht_smooth_pencil: tile side " + std::to_string(n) +
@@ -1126,12 +1129,14 @@ static int smooth_tile_impl(ht_ctx* ctx, const void* d_delta_k, float* d_out, in
 
 extern "C" HT_API int ht_smooth_tile(ht_ctx* ctx, const void* d_delta_k, float* d_out, int n,
                                      double boxsize, double Rf, int wsmooth, void* stream) {
+    HT_RANGE("ht_smooth_tile");
     return smooth_tile_impl(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, 0, n, stream);
 }
 
 extern "C" HT_API int ht_smooth_tile_planes(ht_ctx* ctx, const void* d_delta_k, float* d_out,
                                             int n, double boxsize, double Rf, int wsmooth,
                                             int z_lo, int z_hi, void* stream) {
+    HT_RANGE("ht_smooth_tile_planes");
     return smooth_tile_impl(ctx, d_delta_k, d_out, n, boxsize, Rf, wsmooth, z_lo, z_hi, stream);
 }
 
@@ -1168,6 +1173,7 @@ __global__ void __launch_bounds__(128) wrap_pad_kernel(const float* __restrict__
 extern "C" HT_API int ht_smooth_filter(ht_ctx* ctx, const void* d_delta_k, float* d_tile, int n,
                                        int nbuff, double boxsize, double Rf, int wsmooth,
                                        void* stream) {
+    HT_RANGE("ht_smooth_filter");
     if (!ctx || !d_delta_k || !d_tile) return ht_fail(HT_ERR_INVALID, "ht_smooth_filter: NULL argument");
     if (n < 2 || n > 4096 || nbuff < 0 || nbuff > n)
         return ht_fail(HT_ERR_INVALID, "ht_smooth_filter: need 2 <= n <= 4096 and 0 <= nbuff <= n");

@@ -322,6 +322,20 @@ class HaloFinder:
         check(_lib.load().ht_last_launch_stats(self._h, C.byref(k), C.byref(s), C.byref(c)))
         return {"kernels": k.value, "shells_walked": s.value, "cells_walked": c.value}
 
+    def reject_counts(self) -> dict:
+        """get_dump_counts (RadialShell.jl:28-32): why peaks ended without collapse, summed
+        over every shell analysis on this finder since reset_reject_counts (synchronises
+        the device).  Keys: premask, no_fcrit, m0_one, no_collapse, rthl_neg (the
+        reference's counters) and outside (centres outside the bound tile)."""
+        n = len(_lib.REJECT_REASONS)
+        v = (C.c_int64 * n)()
+        check(_lib.load().ht_reject_counts(self._h, v))
+        return dict(zip(_lib.REJECT_REASONS, (int(x) for x in v)))
+
+    def reset_reject_counts(self, stream=None) -> None:
+        """reset_dump_counters! (RadialShell.jl:19-26), stream-ordered."""
+        check(_lib.load().ht_reset_reject_counts(self._h, _stream_handle(stream)))
+
     def tune(self, block_bits: Optional[int] = None, pf_kz: Optional[int] = None,
              walk_bpsm: Optional[int] = None, fft_path: Optional[int] = None,
              wait_ns: Optional[int] = None, inject_tx: Optional[int] = None) -> None:

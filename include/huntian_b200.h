@@ -470,6 +470,35 @@ HT_API int ht_bracket_adam(ht_ctx* ctx, float* d_params, const float* d_grads, f
 HT_API int ht_last_launch_stats(const ht_ctx* ctx, int64_t* kernels, int64_t* shells_walked,
                          int64_t* cells_walked);
 
+/* Reject-reason counters of the shell collapse: why a peak ended without collapse, the
+ * counters of RadialShell.jl:13-32 (bumped at RadialShell.jl:310,517,604,684,698) kept per
+ * context on the device.  Every ht_shell_analyse and ht_shell_analyse_static call adds to
+ * them (one count per rejected peak) until ht_reset_reject_counts, as the reference's
+ * atomics accumulate until reset_dump_counters!.
+ *   HT_REJECT_PREMASK      masked by a larger halo before the walk (HT_CONV_CPU with
+ *                          rmax2rs > 0 only, which the device path rejects: stays 0)
+ *   HT_REJECT_NO_FCRIT     no shell with Fbar >= fcrit inward of the start (:517)
+ *   HT_REJECT_M0_ONE       the crossing is the centre shell (:604)
+ *   HT_REJECT_NO_COLLAPSE  no shell reaches zvir >= ZZon (:684); also a hunt radius that
+ *                          holds fewer than two shells
+ *   HT_REJECT_RTHL_NEG     the interpolated radius is not positive (:698)
+ *   HT_REJECT_OUTSIDE      the peak's centre lies outside the bound tile (no reference
+ *                          counterpart: the reference would index out of bounds) */
+#define HT_REJECT_PREMASK 0
+#define HT_REJECT_NO_FCRIT 1
+#define HT_REJECT_M0_ONE 2
+#define HT_REJECT_NO_COLLAPSE 3
+#define HT_REJECT_RTHL_NEG 4
+#define HT_REJECT_OUTSIDE 5
+#define HT_REJECT_COUNT 6
+
+/* counts[HT_REJECT_COUNT]: the counters (get_dump_counts, RadialShell.jl:28-32), after the
+ * context's work so far has finished (synchronises the device). */
+HT_API int ht_reject_counts(const ht_ctx* ctx, int64_t* counts);
+/* Zeroes the counters (reset_dump_counters!, RadialShell.jl:19-26), stream-ordered after
+ * the work already issued on `stream` (NULL: the legacy default stream). */
+HT_API int ht_reset_reject_counts(ht_ctx* ctx, void* stream);
+
 /* Measurement aid (no reference counterpart): gathers the packed cell records of the bound
  * tile (ht_fields_pack) at n_idx caller-given cell indices (0-based linear, each < n^3),
  * with the 256-bit record load the shell walk uses, and writes the sum of each record's
@@ -483,8 +512,10 @@ HT_API int ht_record_gather_probe(ht_ctx* ctx, const int64_t* d_idx, int64_t n_i
 /* Device status of the context since the last call (no reference counterpart: the
  * reference kernels have no waits).  Synchronises the device, then returns 0 in *status
  * when every bounded wait of this context's kernels completed, or 1 when a pipeline wait
- * of the peak scan gave up after 2 s (that filter's peaks are then incomplete); the word
- * is cleared on read. */
+ * of the peak scan or of the pencil smoothing gave up (after HT_TUNE_WAIT_NS, 2 s by
+ * default: that filter's output is then incomplete), or 2 when a build with -DHT_CHECKED
+ * (libhuntian_b200_checked.so) found a data-dependent index outside its array and skipped
+ * the access; the word is cleared on read. */
 HT_API int ht_device_status(ht_ctx* ctx, int32_t* status);
 
 /* ---------------------------------------------------- collapse-table generation ---- */

@@ -133,9 +133,11 @@ def make_box_workload(ht, n, L, nbuff, nf, rmin, rmax, seed, max_peaks=1 << 23):
             "fidx": fidx, "Rf_all": Rf_all, "ir2_all": ir2_all, "args": args}
 
 
-def oracle_sample(oracle, W, sel, kind, exact_products=False):
+def oracle_sample(oracle, W, sel, kind, exact_products=False, with_codes=False):
     """Oracle results (and its time in seconds) for the peaks `sel` of a workload;
-    exact_products: the full-FP64 variant (cell products formed exactly)."""
+    exact_products: the full-FP64 variant (cell products formed exactly); with_codes: also
+    return the per-peak reject codes (0 collapsed, 1 premask, 2 no fcrit crossing,
+    3 m0 = 1, 4 no collapse, 5 RTHL <= 0)."""
     import time
     host = {k: v.cpu().numpy() for k, v in W["tile"].items()}
     F = oracle.Fields(host["delta"], host["etax"], host["etay"], host["etaz"], host["eta2x"],
@@ -146,10 +148,12 @@ def oracle_sample(oracle, W, sel, kind, exact_products=False):
     pi, pj, pk = (p[c][:n].cpu().numpy()[sel] for c in ("i", "j", "k"))
     fi = W["fidx"].cpu().numpy()[sel]
     t0 = time.perf_counter()
-    o, _ = oracle.analyse_batch(F, pi, pj, pk, W["ir2_all"].cpu().numpy()[fi],
+    o, codes = oracle.analyse_batch(F, pi, pj, pk, W["ir2_all"].cpu().numpy()[fi],
                                 W["Rf_all"].cpu().numpy()[fi], 1.0, np.float32(W["fcrit"]),
                                 W["alatt"], ct, oracle.precompute_shells(W["finder"].nhunt),
                                 nbuff=W["nbuff"], kind=kind, exact_products=exact_products)
+    if with_codes:
+        return o, time.perf_counter() - t0, codes
     return o, time.perf_counter() - t0
 
 
