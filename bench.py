@@ -984,13 +984,15 @@ def run_reference(args, rank, world, device):
     return line
 
 
-COLLAPSE_METRIC = "ellipsoids/s thru RK4 collapse-table generation"
+def _collapse_metric(solver):
+    name = "RK4" if solver == "rk4" else "Tsit5"
+    return f"ellipsoids/s thru {name} collapse-table generation"
 
 
-def _collapse_setup(ht):
+def _collapse_setup(ht, solver="rk4"):
     col, cat = ht.collapse, ht.catalog
     cp = cat.CosmologyParams(Om=0.315, OB=0.049, OL=0.685, h=0.674, ns=0.965, s8=0.808)
-    ep = col.EllipsoidParams(cp)
+    ep = col.EllipsoidParams(cp, solver=solver)
     tp = col.CollapseTableParams()
     return cp, ep, tp
 
@@ -998,14 +1000,14 @@ def _collapse_setup(ht):
 def _collapse_cpu(ep, tp):
     """The oracle's make_table (C restatement, OpenMP on every host thread), once."""
     from oracle import collapse as oc, max_threads
-    eo = oc.EllipsoidOracle(ep.dlin_tables, ep.cosmo.Om, ep.cosmo.OL)
+    eo = oc.EllipsoidOracle(ep.dlin_tables, ep.cosmo.Om, ep.cosmo.OL, solver=ep.solver)
     t0 = time.perf_counter()
     eo.make_table(tp.Nx, tp.Ny, tp.Nz, *tp.axes)
     dt = time.perf_counter() - t0
     n = tp.Nx * tp.Ny * tp.Nz
     return {"value": n / dt, "unit": "ellipsoids/s", "cores": max_threads(), "kind": "port",
             "sample": f"the whole {tp.Nx}x{tp.Ny}x{tp.Nz} table ({n} ellipsoids), or_make_table "
-                      f"(C restatement of the RK4 path, FP64, OpenMP)"}
+                      f"(C restatement of the {ep.solver} path, FP64, OpenMP)"}
 
 
 def run_collapse_table(args, rank, world, device):
@@ -1015,11 +1017,14 @@ def run_collapse_table(args, rank, world, device):
     ht_collapse_table (grid upload, launch, table download) timed around each call."""
     import torch
     ht = _package()
-    cp, ep, tp = _collapse_setup(ht)
+    cp, ep, tp = _collapse_setup(ht, args.solver)
     n = tp.Nx * tp.Ny * tp.Nz
-    config = {"workload": "collapse_table",
+    integ = ("RK4 tfac 0.01, nstepmax 10000" if args.solver == "rk4" else
+             "Tsit5 abstol 1e-8 reltol 1e-6 (the reference's default :diffeq)")
+    metric = _collapse_metric(args.solver)
+    config = {"workload": "collapse_table", "solver": args.solver,
               "desc": f"{tp.Nx}x{tp.Ny}x{tp.Nz} zvir table (log10 Frho, e_v, p_v/e_v), "
-                      "RK4 tfac 0.01, nstepmax 10000, Planck 2018 (Om 0.315, OL 0.685)",
+                      f"{integ}, Planck 2018 (Om 0.315, OL 0.685)",
               "ellipsoids_per_step": n, "l2": "inputs 480 KB: compute bound, no flush",
               "parallelism": f"replicas x{world}"}
     if args.impl == "reference":
@@ -1029,7 +1034,7 @@ def run_collapse_table(args, rank, world, device):
         v = float(np.mean([c["value"] for c in vals]))
         cb = dict(vals[-1])
         cb["value"] = v
-        return {"metric": COLLAPSE_METRIC, "value": v, "unit": "ellipsoids/s", "n_gpus": world,
+        return {"metric": metric, "value": v, "unit": "ellipsoids/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * n / v,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (the table's own grid)", "config": config,
@@ -1072,7 +1077,7 @@ def run_collapse_table(args, rank, world, device):
         wall.append(time.perf_counter() - t0)
     e2e_s = float(np.median(wall))
     ntab = len(ep.dlin_tables.atab)
-    line = {"metric": COLLAPSE_METRIC, "value": world * n / (ms / 1e3), "unit": "ellipsoids/s",
+    line = {"metric": metric, "value": world * n / (ms / 1e3), "unit": "ellipsoids/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (the table's own grid)", "config": config,
@@ -1097,6 +1102,8 @@ def main():
     ap.add_argument("--workload", default="tile1152",
                     choices=list(WORKLOADS) + ["collapse_table"])
     ap.add_argument("--mode", default="learned", choices=["learned", "batched", "plain"])
+    ap.add_argument("--solver", default="rk4", choices=["rk4", "diffeq"],
+                    help="collapse_table workload: the integrator (the reference's two)")
     ap.add_argument("--graph", type=int, default=1,
                     help="capture the per-filter smoothing + peak-scan loop in a CUDA graph")
     ap.add_argument("--autotune", type=int, default=1,

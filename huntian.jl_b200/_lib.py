@@ -105,7 +105,11 @@ class HtCosmo(C.Structure):
 class HtEllipsoid(C.Structure):
     _fields_ = [("Om", C.c_double), ("OL", C.c_double), ("iforce_strat", C.c_int32),
                 ("ivir_strat", C.c_int32), ("fcoll", C.c_double * 3), ("tfac", C.c_double),
-                ("nstepmax", C.c_int32), ("zinit_fac", C.c_double)]
+                ("nstepmax", C.c_int32), ("zinit_fac", C.c_double), ("solver", C.c_int32)]
+
+
+HT_SOLVER_RK4 = 0
+HT_SOLVER_TSIT5 = 1
 
 
 class HtGrowth(C.Structure):

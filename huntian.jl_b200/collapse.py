@@ -3,11 +3,13 @@ ht_collapse_table, mirroring the reference's EllipsoidalCollapse / CollapseTable
 (src/EllipsoidalCollapse/EllipsoidalCollapse.jl, src/EllipsoidalCollapse/CollapseTable.jl,
 bin/generate_table.jl).
 
-The integrator is the reference's fixed-step RK4 path (`solver = :rk4`, the port of the
-Fortran HomogeneousEllipsoid.f90), one ellipsoid per device thread in FP64.  The reference's
-default `:diffeq` path (OrdinaryDiffEq's adaptive Tsit5) is not restated: asking for it
-raises.  Tables come out in this package's HomelTab layout, (nz, ny, nx) float32 holding
-Julia's column-major bytes, ready for write_homeltab / HaloFinder.
+Both of the reference's integrators run on the device, one ellipsoid per thread in FP64:
+`solver = "diffeq"` (the reference's default, `_evolve_diffeq`, EllipsoidalCollapse.jl:
+440-485: adaptive Tsit5 with abstol 1e-8, reltol 1e-6 and OrdinaryDiffEq's step control,
+restated from the published method) and `solver = "rk4"` (the fixed-step port of the
+Fortran HomogeneousEllipsoid.f90, which reproduces the shipped HomelTab tables).  Tables
+come out in this package's HomelTab layout, (nz, ny, nx) float32 holding Julia's
+column-major bytes, ready for write_homeltab / HaloFinder.
 """
 from __future__ import annotations
 
@@ -37,13 +39,13 @@ class EllipsoidParams:
     nstepmax: int = 10000
     zinit_fac: float = 20.0
     iwant_rd: int = 1
-    solver: str = "rk4"
+    solver: str = "diffeq"
     dlin_tables: Optional[DlinearTables] = field(default=None, repr=False)
 
     def __post_init__(self):
-        if self.solver not in ("rk4",):
-            raise ValueError(f"solver {self.solver!r}: only the fixed-step 'rk4' path "
-                             "(EllipsoidalCollapse.jl:492-590) is implemented")
+        if self.solver not in ("rk4", "diffeq"):
+            raise ValueError(f"solver {self.solver!r}: 'diffeq' (adaptive Tsit5) or 'rk4' "
+                             "(the fixed-step Fortran path), as EllipsoidalCollapse.jl:23")
         if self.iwant_rd != 1:
             raise ValueError("iwant_rd != 1 (Legendre form) is not implemented, as in the "
                              "reference")
@@ -53,7 +55,8 @@ class EllipsoidParams:
     def _structs(self):
         e = HtEllipsoid(self.cosmo.Om, self.cosmo.OL, self.iforce_strat, self.ivir_strat,
                         (C.c_double * 3)(self.fcoll_1, self.fcoll_2, self.fcoll_3), self.tfac,
-                        self.nstepmax, self.zinit_fac)
+                        self.nstepmax, self.zinit_fac,
+                        _lib.HT_SOLVER_TSIT5 if self.solver == "diffeq" else _lib.HT_SOLVER_RK4)
         g = self.dlin_tables
         keep = [np.ascontiguousarray(a, np.float64)
                 for a in (g.atab, g.D_atab, g.dlnD_dlnatab)]
@@ -124,12 +127,12 @@ def make_table(ep: EllipsoidParams, tp: Optional[CollapseTableParams] = None,
 
 
 def generate_table(path: str, Om: float = 0.315, OB: float = 0.049, OL: float = 0.685,
-                   h: float = 0.674, device: int = 0) -> np.ndarray:
-    """bin/generate_table.jl --solver rk4: the default 50 x 20 x 20 table for the given
-    cosmology, written as a HomelTab file."""
+                   h: float = 0.674, solver: str = "diffeq", device: int = 0) -> np.ndarray:
+    """bin/generate_table.jl [--solver diffeq|rk4]: the default 50 x 20 x 20 table for the
+    given cosmology, written as a HomelTab file."""
     from .tables import write_homeltab
     cosmo = CosmologyParams(Om=Om, OB=OB, OL=OL, h=h, ns=0.965, s8=0.808)
     tp = CollapseTableParams()
-    t = make_table(EllipsoidParams(cosmo), tp, device)
+    t = make_table(EllipsoidParams(cosmo, solver=solver), tp, device)
     write_homeltab(path, t, tp.axes)
     return t

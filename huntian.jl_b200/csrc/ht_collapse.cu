@@ -1,15 +1,16 @@
 // Collapse-table generation on the device: homogeneous-ellipsoid collapse with the
 // reference's fixed-step "funny RK4" (EllipsoidalCollapse.jl:149-590 with solver = :rk4,
-// the port of the Fortran HomogeneousEllipsoid.f90) for many (Frho, e_v, p_v) at once,
-// and the zvir table of CollapseTable.jl:22-76 built from it.
+// the port of the Fortran HomogeneousEllipsoid.f90) or its adaptive Tsit5 path (solver =
+// :diffeq, :333-485) for many (Frho, e_v, p_v) at once, and the zvir table of
+// CollapseTable.jl:22-76 built from either.
 //
 // One thread integrates one ellipsoid in FP64; the entries are independent (20,000 for the
 // 50 x 20 x 20 table).  The integration is a dependent chain of ~10^3 RK4 steps, each four
 // right-hand sides with two Carlson RD evaluations (square-root chains): latency bound, so
 // the launch uses small CTAs to spread the threads over every SM.  This file is compiled
 // with -fmad=false: no product is fused into an addition, the operations run in the
-// reference's order, and the results follow the CPU restatement to the last bit except
-// where the library log of the oblate shape branch differs by an ulp.
+// reference's order, and the one logarithm on the path (the oblate shape branch) is a
+// series both sides carry, so the results follow the CPU restatement to the last bit.
 #include <cmath>
 #include <vector>
 
@@ -177,6 +178,23 @@ __device__ void elliptic_rd2(double x1, double y1, double z1, double x2, double 
     *r2 = rd_final(b);
 }
 
+// Natural log of a finite x > 0 (and log2 x through log2x when non-null): x = m 2^e with m
+// in [1/sqrt 2, sqrt 2), log x = e ln 2 + 2 atanh((m - 1)/(m + 1)), the atanh series summed
+// to the 23rd power.  The CPU restatement carries the same function, operation for
+// operation, so that both round alike (library logs may differ in the last bit, which the
+// adaptive path would amplify into a different step sequence).
+__device__ double log_series(double x, double* log2x) {
+    int ex;
+    double m = frexp(x, &ex);
+    if (m < 0.7071067811865476) { m *= 2.0; ex -= 1; }
+    const double s = (m - 1.0) / (m + 1.0), s2 = s * s;
+    double t = 1.0 / 23.0;
+    for (int k = 21; k >= 1; k -= 2) t = 1.0 / (double)k + s2 * t;
+    const double lnm = 2.0 * s * t;
+    if (log2x) *log2x = (double)ex + lnm * 1.4426950408889634;
+    return (double)ex * 0.6931471805599453 + lnm;
+}
+
 // Shape integrals (EllipsoidalCollapse.jl:108-146, iwant_rd = 1).
 __device__ void get_b_2(double a1, double a2, double a3, double* b) {
     const double third = 1.0 / 3.0;
@@ -191,11 +209,12 @@ __device__ void get_b_2(double a1, double a2, double a3, double* b) {
             const double ecc2 = 1.0 - r_3 * r_3, one_ecc2 = r_3 * r_3,
                          one_ecc = 0.5 * (r_3 * r_3), ecc = sqrt(ecc2);
             b3 = 0.5 * (one_ecc2 / ecc2 *
-                        (1.0 / one_ecc2 - log((1.0 + ecc) / one_ecc) * 0.5 / ecc));
+                        (1.0 / one_ecc2 - log_series((1.0 + ecc) / one_ecc, nullptr) * 0.5 / ecc));
         } else {
             const double ecc2 = 1.0 - r_3 * r_3, ecc = sqrt(ecc2);
             b3 = 0.5 * ((1.0 - ecc2) / ecc2 *
-                        (1.0 / (1.0 - ecc2) - log((1.0 + ecc) / (1.0 - ecc)) * 0.5 / ecc));
+                        (1.0 / (1.0 - ecc2) -
+                         log_series((1.0 + ecc) / (1.0 - ecc), nullptr) * 0.5 / ecc));
         }
         b[0] = 1.0 - 2.0 * b3;
         b[1] = b3;
@@ -394,6 +413,251 @@ __global__ void __launch_bounds__(kEvolveThreads) evolve_kernel(
     if (steps_out) steps_out[q] = istep;
 }
 
+// ---------------------------------- solver = :diffeq: adaptive Tsit5 (:333-485) ----
+//
+// The same integrator as the CPU restatement (oracle or_evolve_tsit5), operation for
+// operation, so that both take the same steps: Tsitouras' 5(4) pair with OrdinaryDiffEq's
+// controls (starting step of Hairer, Norsett & Wanner; RMS error norm with abstol 1e-8,
+// reltol 1e-6; PI controller beta1 = 7/50, beta2 = 2/25, safety 9/10, step ratio in
+// [1/10, 5]; at most 100,000 iterations), stopping after the first accepted step at which
+// axis 1 has virialised.
+
+// x^y for finite x > 0: 2^(y log2 x), log2 x from log_series and 2^f from its Taylor
+// series (about 1e-15 relative); plain arithmetic, so the host restatement rounds alike.
+__device__ double pow_pos(double x, double y) {
+    double l2;
+    log_series(x, &l2);
+    const double v = y * l2;
+    const double nn = floor(v + 0.5);
+    const double f = (v - nn) * 0.6931471805599453;
+    double p = 1.0;
+    for (int k = 16; k >= 1; --k) p = 1.0 + f * p / (double)k;
+    return ldexp(p, (int)nn);
+}
+
+// VirState (EllipsoidalCollapse.jl:327-333), with the growth-table lookup hint.
+struct VirDev {
+    int lvirv[3];
+    int hint;
+    double a_eq[3], zdynv[3];
+};
+
+// _diffeq_rhs! (EllipsoidalCollapse.jl:344-438): du at (t, u); freezes the virialised axes
+// in u and advances the flags at every evaluation (accepted step or not), recording 1/a at
+// the evaluation that sets each.  aLam[3] = Frho / 3; iforce_strat 2 keeps the velocities.
+__device__ void diffeq_rhs(const EllDev& e, const GrowthDev& g, const double* aLam, double t,
+                           double* u, double* du, VirDev& v) {
+    const double a_b = t, a_b3 = a_b * a_b * a_b;
+    const double Ha = ha_b_nr(a_b, e);
+    const double Ha_inv = 1.0 / Ha;
+    if (v.lvirv[2] == 0 && u[2] <= e.fcoll[2] * a_b) {
+        v.lvirv[2] = 1;
+        v.a_eq[2] = e.fcoll[2] * a_b;
+        v.zdynv[2] = 1.0 / a_b;
+    }
+    double a_3eq2 = 0.0, a_3eq1 = 0.0;
+    if (e.vs == 2 && v.lvirv[1] == 0) a_3eq2 = e.fcoll[1] * a_b;
+    else if (e.vs == 1 && v.lvirv[2] == 1) a_3eq2 = v.a_eq[2] * 1.001;
+    if (e.vs == 2 && v.lvirv[0] == 0) a_3eq1 = e.fcoll[0] * a_b;
+    else if (e.vs == 1 && v.lvirv[2] == 1) a_3eq1 = v.a_eq[2] * 1.0003;
+    if (v.lvirv[2] == 1 && v.lvirv[1] == 0 && u[1] <= a_3eq2) {
+        v.lvirv[1] = 1;
+        v.a_eq[1] = a_3eq2;
+        v.zdynv[1] = 1.0 / a_b;
+    }
+    if (v.lvirv[2] == 1 && v.lvirv[0] == 0 && u[0] <= a_3eq1) {
+        v.lvirv[0] = 1;
+        v.a_eq[0] = a_3eq1;
+        v.zdynv[0] = 1.0 / a_b;
+    }
+#pragma unroll
+    for (int ax = 2; ax >= 0; --ax)
+        if (v.lvirv[ax] == 1) { u[ax] = v.a_eq[ax]; u[ax + 3] = 0.0; }
+
+    const double a1 = u[0], a2 = u[1], a3 = u[2];
+    const double delta1_e = a_b3 / (a1 * a2 * a3);
+    const double Frho_3 = aLam[3];
+    double d0, d1_int, d1_ext = 0.0;
+    if (e.fs == 0) {
+        d0 = -e.Rvac * Ha_inv;
+        d1_int = 1.5 * delta1_e / a_b3 * Ha_inv;
+    } else {
+        d0 = (0.5 / a_b3 - e.Rvac) * Ha_inv;
+        d1_int = 1.5 * (delta1_e - 1.0) / a_b3 * Ha_inv;
+        if (e.fs == 4 || e.fs == 5 || e.fs == 6) {
+            double dlin, hd;
+            dlinear_ab(g, a_b, &dlin, &hd, &v.hint);
+            d1_ext = 1.5 / a_b3 * Ha_inv * dlin;
+        } else if (e.fs == 3) {
+            d1_ext = 1.5 * 2.5 / a_b3 * Ha_inv;
+        }
+    }
+    double b[3] = {0.0, 0.0, 0.0};
+    if (e.fs != 5 && e.fs != 6) get_b_2(a1, a2, a3, b);
+    const double third = 1.0 / 3.0;
+#pragma unroll
+    for (int ax = 0; ax < 3; ++ax) {
+        if (v.lvirv[ax] == 1) { du[ax] = 0.0; du[ax + 3] = 0.0; continue; }
+        du[ax] = u[ax + 3] * Ha_inv;
+        double f = 0.0;
+        if (e.fs == 0) f = -u[ax] * d1_int * b[ax];
+        else if (e.fs == 1) f = -u[ax] * (d1_int * b[ax] + d0);
+        else if (e.fs == 3) f = -u[ax] * (d1_int * b[ax] + d0 + d1_ext * (b[ax] - third));
+        else if (e.fs == 4 || e.fs == 6)
+            f = -u[ax] * (d1_int * b[ax] + d0 + d1_ext * (aLam[ax] - Frho_3));
+        else if (e.fs == 5) f = -u[ax] * d0 - d1_ext * a_b * aLam[ax];
+        du[ax + 3] = f;
+    }
+}
+
+// Tsitouras' 5(4) pair (Comput. Math. Appl. 62 (2011) 770-775) in OrdinaryDiffEq's
+// tabulation: nodes, stage weights (row 7 = the solution weights, first same as last) and
+// the weights of the embedded error estimate.
+__constant__ double kTsC[7] = {0.0, 0.161, 0.327, 0.9, 0.9800255409045097, 1.0, 1.0};
+__constant__ double kTsA[7][6] = {
+    {0, 0, 0, 0, 0, 0},
+    {0.161, 0, 0, 0, 0, 0},
+    {-0.008480655492356989, 0.335480655492357, 0, 0, 0, 0},
+    {2.897153057105493, -6.359448489975075, 4.3622954328695815, 0, 0, 0},
+    {5.325864828439257, -11.748883564062828, 7.4955393428898365, -0.09249506636175525, 0, 0},
+    {5.86145544294642, -12.92096931784711, 8.159367898576159, -0.071584973281401,
+     -0.028269050394068383, 0},
+    {0.09646076681806523, 0.01, 0.4798896504144996, 1.379008574103742, -3.290069515436081,
+     2.324710524099774}};
+__constant__ double kTsE[7] = {-0.00178001105222577714, -0.0008164344596567469,
+                               0.007880878010261995, -0.1447110071732629,
+                               0.5823571654525552, -0.45808210592918697,
+                               0.015151515151515152};
+
+__device__ double rms6(const double* v) {
+    double s = 0.0;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s += v[i] * v[i];
+    return sqrt(s / 6.0);
+}
+
+// _evolve_diffeq (EllipsoidalCollapse.jl:440-485), one ellipsoid per thread: zvir = 1/a at
+// axis idynax's virialisation (1-3), D(a) there and Frho D, all -1 without the event
+// before a = 2.  steps_out: the iterations (accepted and rejected steps).
+__global__ void __launch_bounds__(kEvolveThreads) evolve_tsit5_kernel(
+    const EllDev e, const GrowthDev g, long long n, const double* __restrict__ Frho_in,
+    const double* __restrict__ ev_in, const double* __restrict__ pv_in, int idynax,
+    double* __restrict__ zout, double* __restrict__ Dout, double* __restrict__ fcout,
+    int32_t* __restrict__ steps_out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const double Frho = Frho_in[q], e_v = ev_in[q], p_v = pv_in[q];
+    const double abstol = 1e-8, reltol = 1e-6, tend = 2.0;
+    const int maxiters = 100000;
+    double aLam[4];
+    aLam[2] = Frho / 3.0 * (1.0 + 3.0 * e_v + p_v);
+    aLam[1] = Frho / 3.0 * (1.0 - 2.0 * p_v);
+    aLam[0] = Frho / 3.0 * (1.0 - 3.0 * e_v + p_v);
+    aLam[3] = Frho / 3.0;
+    VirDev v;
+    v.hint = 0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) { v.lvirv[i] = 0; v.a_eq[i] = 0.0; v.zdynv[i] = -1.0; }
+    const double zinit = e.zinit_fac * Frho;
+    const double a_b = 1.0 / zinit;
+    double dlin, HD_Ha;
+    dlinear_ab(g, a_b, &dlin, &HD_Ha, &v.hint);
+    const double Ha = ha_b_nr(a_b, e);
+    double u[6];
+#pragma unroll
+    for (int ax = 2; ax >= 0; --ax) u[ax] = a_b * (1.0 - dlin * aLam[ax]);
+#pragma unroll
+    for (int ax = 2; ax >= 0; --ax) u[ax + 3] = Ha * (1.0 - (1.0 + HD_Ha) * dlin * aLam[ax]);
+    double t = a_b;
+
+    double k[7][6], tmp[6], sc[6], u1[6];
+    diffeq_rhs(e, g, aLam, t, u, k[0], v);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) sc[i] = abstol + fabs(u[i]) * reltol;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) tmp[i] = u[i] / sc[i];
+    const double d0 = rms6(tmp);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) tmp[i] = k[0][i] / sc[i];
+    const double d1 = rms6(tmp);
+    double dt0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * (d0 / d1);
+    if (dt0 > tend - t) dt0 = tend - t;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) u1[i] = u[i] + dt0 * k[0][i];
+    diffeq_rhs(e, g, aLam, t + dt0, u1, k[1], v);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) tmp[i] = (k[1][i] - k[0][i]) / sc[i];
+    const double d2 = rms6(tmp) / dt0;
+    const double dmax = d1 > d2 ? d1 : d2;
+    const double dt1 = dmax <= 1e-15 ? (1e-6 > dt0 * 1e-3 ? 1e-6 : dt0 * 1e-3)
+                                     : pow_pos(0.01 / dmax, 0.2);
+    double dt = 100.0 * dt0 < dt1 ? 100.0 * dt0 : dt1;
+    if (dt > tend - t) dt = tend - t;
+    diffeq_rhs(e, g, aLam, t, u, k[0], v);   // the first FSAL stage
+
+    double qold = 1e-4;
+    int iter = 0;
+    // bounded: every round advances iter, and the loop ends at maxiters
+    while (iter < maxiters && t < tend) {
+        ++iter;
+        if (dt > tend - t) dt = tend - t;
+        if (!(dt > 1e-14 * t)) break;   // step size underflow: give up
+        for (int st = 1; st < 7; ++st) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                double acc = 0.0;
+                for (int j = 0; j < st; ++j) acc += kTsA[st][j] * k[j][i];
+                tmp[i] = u[i] + dt * acc;
+            }
+            diffeq_rhs(e, g, aLam, t + kTsC[st] * dt, tmp, k[st], v);
+        }
+        // tmp is the step's end, frozen by the last evaluation
+        double r[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 0; j < 7; ++j) acc += kTsE[j] * k[j][i];
+            const double au = fabs(u[i]), an = fabs(tmp[i]);
+            r[i] = (dt * acc) / (abstol + (au > an ? au : an) * reltol);
+        }
+        const double EEst = rms6(r);
+        if (EEst <= 1.0) {
+            double qq;
+            if (EEst == 0.0) {
+                qq = 0.1;
+            } else {
+                qq = pow_pos(EEst, 0.14) / pow_pos(qold, 0.08) / 0.9;
+                qq = qq < 5.0 ? qq : 5.0;
+                qq = qq > 0.1 ? qq : 0.1;
+            }
+            t = t + dt;
+            if (tend - t <= 1e-13 * tend) t = tend;
+#pragma unroll
+            for (int i = 0; i < 6; ++i) { u[i] = tmp[i]; k[0][i] = k[6][i]; }
+            qold = EEst > 1e-4 ? EEst : 1e-4;
+            dt = dt / qq;
+            if (v.lvirv[0] == 1) break;   // the terminating callback
+        } else {
+            const double q11 = EEst == EEst ? pow_pos(EEst, 0.14) / 0.9 : 5.0;
+            dt = dt / (q11 < 5.0 ? q11 : 5.0);
+        }
+    }
+    double z = -1.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+        if (i == idynax - 1) z = v.zdynv[i];
+    double D = -1.0, fc = -1.0;
+    if (z != -1.0) {
+        D = dfnofa(g, 1.0 / z);
+        fc = Frho * D;
+    }
+    zout[q] = z;
+    if (Dout) Dout[q] = D;
+    if (fcout) fcout[q] = fc;
+    if (steps_out) steps_out[q] = iter;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------- host side ----
@@ -408,6 +672,8 @@ int check_inputs(const ht_ellipsoid* ep, const ht_growth* g, const char* who) {
         return ht_fail(HT_ERR_INVALID, w + ": iforce_strat must be in 0..6");
     if (ep->ivir_strat != 1 && ep->ivir_strat != 2)
         return ht_fail(HT_ERR_INVALID, w + ": ivir_strat must be 1 or 2");
+    if (ep->solver != HT_SOLVER_RK4 && ep->solver != HT_SOLVER_TSIT5)
+        return ht_fail(HT_ERR_INVALID, w + ": solver must be HT_SOLVER_RK4 or HT_SOLVER_TSIT5");
     if (ep->nstepmax < 1 || ep->nstepmax > 100000000)
         return ht_fail(HT_ERR_INVALID, w + ": nstepmax must be in 1..10^8");
     if (!(ep->tfac > 0.0) || !(ep->zinit_fac > 0.0))
@@ -448,6 +714,10 @@ extern "C" HT_API int ht_evolve_ellipses(int device, const ht_ellipsoid* ep,
     if (n < 0) return ht_fail(HT_ERR_INVALID, "ht_evolve_ellipses: n < 0");
     if (idynax < 1 || idynax > 6)
         return ht_fail(HT_ERR_INVALID, "ht_evolve_ellipses: idynax must be in 1..6");
+    if (ep->solver == HT_SOLVER_TSIT5 && idynax > 3)
+        return ht_fail(HT_ERR_INVALID,
+                       "ht_evolve_ellipses: the Tsit5 path records axis virialisation only "
+                       "(idynax 1..3)");
     if (n == 0) return HT_OK;
     if (!d_Frho || !d_e_v || !d_p_v || !d_zvir)
         return ht_fail(HT_ERR_INVALID, "ht_evolve_ellipses: NULL input or output array");
@@ -466,9 +736,14 @@ extern "C" HT_API int ht_evolve_ellipses(int device, const ht_ellipsoid* ep,
         GrowthDev g{buf, buf + nt, buf + 2 * nt, nt, growth->amintab, growth->amaxtab,
                     growth->D_ainfty, growth->D_a0, growth->HD_Hainfty, growth->HD_Ha0};
         const long long blocks = (n + kEvolveThreads - 1) / kEvolveThreads;
-        evolve_kernel<<<(unsigned)blocks, kEvolveThreads, 0, st>>>(
-            ell_dev(ep), g, (long long)n, d_Frho, d_e_v, d_p_v, idynax, d_zvir, d_D, d_fc,
-            d_steps);
+        if (ep->solver == HT_SOLVER_TSIT5)
+            evolve_tsit5_kernel<<<(unsigned)blocks, kEvolveThreads, 0, st>>>(
+                ell_dev(ep), g, (long long)n, d_Frho, d_e_v, d_p_v, idynax, d_zvir, d_D, d_fc,
+                d_steps);
+        else
+            evolve_kernel<<<(unsigned)blocks, kEvolveThreads, 0, st>>>(
+                ell_dev(ep), g, (long long)n, d_Frho, d_e_v, d_p_v, idynax, d_zvir, d_D, d_fc,
+                d_steps);
         e = cudaGetLastError();
     }
     // stream-ordered release: after the kernel that reads the table

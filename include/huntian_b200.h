@@ -41,9 +41,10 @@
  *   ht_fsc_of_z         -> src/HaloFinder/RadialShell.jl:181-195 `fsc_of_z` (host)
  *   ht_ctx_shell_r2     -> the shell_r2 array of src/ShellAnalysisGPU.jl:44-71
  *   ht_evolve_ellipses  -> src/EllipsoidalCollapse/EllipsoidalCollapse.jl:492-590
- *                          `evolve_ellipse_full` (solver = :rk4), many ellipsoids at once
+ *                          `evolve_ellipse_full` (solver = :rk4, or :diffeq through
+ *                          `_evolve_diffeq` :440-485), many ellipsoids at once
  *   ht_collapse_table   -> src/EllipsoidalCollapse/CollapseTable.jl:29-76 `make_table` /
- *                          `make_table_threaded` (bin/generate_table.jl --solver rk4)
+ *                          `make_table_threaded` (bin/generate_table.jl --solver rk4|diffeq)
  */
 #ifndef HUNTIAN_B200_H
 #define HUNTIAN_B200_H
@@ -522,7 +523,13 @@ HT_API int ht_device_status(ht_ctx* ctx, int32_t* status);
 
 /* EllipsoidParams (src/EllipsoidalCollapse/EllipsoidalCollapse.jl:10-45) with its
  * cosmology's Om and OL; the defaults there are iforce_strat 4, ivir_strat 2, fcoll
- * (0.01, 0.171, 0.171), tfac 0.01, nstepmax 10000, zinit_fac 20. */
+ * (0.01, 0.171, 0.171), tfac 0.01, nstepmax 10000, zinit_fac 20, solver :diffeq.
+ * solver: HT_SOLVER_RK4, the fixed-step RK4 of the Fortran code (tfac, nstepmax; events
+ * 1-6), or HT_SOLVER_TSIT5, the :diffeq path (EllipsoidalCollapse.jl:440-485): Tsit5 with
+ * abstol 1e-8, reltol 1e-6, at most 100,000 iterations, stopping once axis 1 has
+ * virialised (events 1-3; tfac and nstepmax unused). */
+#define HT_SOLVER_RK4 0
+#define HT_SOLVER_TSIT5 1
 typedef struct {
     double Om, OL;
     int32_t iforce_strat;     /* 0, 1, 3, 4, 5 or 6 (2 leaves the velocities constant) */
@@ -531,6 +538,7 @@ typedef struct {
     double tfac;              /* RK4 step factor */
     int32_t nstepmax;         /* step limit, 1 .. 10^8 */
     double zinit_fac;         /* initial 1/a = zinit_fac Frho */
+    int32_t solver;           /* HT_SOLVER_RK4 or HT_SOLVER_TSIT5 */
 } ht_ellipsoid;
 
 /* DlinearTables (src/Cosmology/Cosmology.jl:68-78), HOST arrays of ntab >= 4 entries, atab
@@ -543,11 +551,11 @@ typedef struct {
     double amintab, amaxtab, D_ainfty, D_a0, HD_Hainfty, HD_Ha0;
 } ht_growth;
 
-/* evolve_ellipse_full with the fixed-step RK4 (EllipsoidalCollapse.jl:492-590) for n
- * ellipsoids (DEVICE arrays Frho, e_v, p_v), event idynax (1-3 axis virialisation, 4-6
- * turnaround): d_zvir = 1/a at the event, d_D = D(a) there, d_fc = Frho D, all -1 when the
- * event does not happen before a = 2 or nstepmax steps.  d_D, d_fc and d_steps (steps
- * taken) may be NULL.  One device thread per ellipsoid, FP64.  Asynchronous on `stream`
+/* evolve_ellipse_full (EllipsoidalCollapse.jl:492-590) with ep->solver for n ellipsoids
+ * (DEVICE arrays Frho, e_v, p_v), event idynax (1-3 axis virialisation, 4-6 turnaround,
+ * RK4 only): d_zvir = 1/a at the event, d_D = D(a) there, d_fc = Frho D, all -1 when the
+ * event does not happen before a = 2 (or nstepmax RK4 steps).  d_D, d_fc and d_steps
+ * (steps taken; with Tsit5 accepted and rejected) may be NULL.  One device thread per ellipsoid, FP64.  Asynchronous on `stream`
  * (the growth table is staged to the device in stream order; the host arrays may be
  * released when the call returns). */
 HT_API int ht_evolve_ellipses(int device, const ht_ellipsoid* ep, const ht_growth* growth,

@@ -1,6 +1,7 @@
 """Oracle of the collapse-table generator (test infrastructure): ctypes bindings of
 or_collapse.c, the C restatement of the reference's RK4 homogeneous-ellipsoid collapse
-(EllipsoidalCollapse.jl:149-590 with solver = :rk4) and of the table sweep
+(EllipsoidalCollapse.jl:149-590 with solver = :rk4), of its adaptive Tsit5 path
+(solver = :diffeq, :333-485) and of the table sweep
 (CollapseTable.jl:22-76).  Only the tests and the bench's CPU baseline use it."""
 from __future__ import annotations
 
@@ -22,7 +23,8 @@ class Growth(C.Structure):
 class Ellipsoid(C.Structure):
     _fields_ = [("Om", C.c_double), ("OL", C.c_double), ("iforce_strat", C.c_int),
                 ("ivir_strat", C.c_int), ("fcoll", C.c_double * 3), ("tfac", C.c_double),
-                ("nstepmax", C.c_int), ("zinit_fac", C.c_double), ("growth", Growth)]
+                ("nstepmax", C.c_int), ("zinit_fac", C.c_double), ("growth", Growth),
+                ("solver", C.c_int)]
 
 
 def _declare(L):
@@ -38,6 +40,8 @@ def _declare(L):
     L.or_evolve_ellipse.argtypes = [C.POINTER(Ellipsoid), C.c_double, C.c_double, C.c_double,
                                     C.c_int, C.POINTER(C.c_double)]
     L.or_evolve_ellipse.restype = C.c_int
+    L.or_pow_pos.argtypes = [C.c_double, C.c_double]
+    L.or_pow_pos.restype = C.c_double
     L.or_make_table.argtypes = [C.POINTER(Ellipsoid)] + [C.c_int] * 3 + [C.c_double] * 6 + \
         [C.c_void_p]
     L._collapse_declared = True
@@ -55,15 +59,17 @@ class EllipsoidOracle:
 
     def __init__(self, g, Om: float, OL: float, iforce_strat: int = 4, ivir_strat: int = 2,
                  fcoll=(0.01, 0.171, 0.171), tfac: float = 0.01, nstepmax: int = 10000,
-                 zinit_fac: float = 20.0):
+                 zinit_fac: float = 20.0, solver: str = "rk4"):
         self._keep = [np.ascontiguousarray(g.atab, np.float64),
                       np.ascontiguousarray(g.D_atab, np.float64),
                       np.ascontiguousarray(g.dlnD_dlnatab, np.float64)]
         P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
         gr = Growth(P(self._keep[0]), P(self._keep[1]), P(self._keep[2]), len(self._keep[0]),
                     g.amintab, g.amaxtab, g.D_ainfty, g.D_a0, g.HD_Hainfty, g.HD_Ha0)
+        if solver not in ("rk4", "diffeq"):
+            raise ValueError(f"solver {solver!r}: 'rk4' or 'diffeq'")
         self.s = Ellipsoid(Om, OL, iforce_strat, ivir_strat, (C.c_double * 3)(*fcoll), tfac,
-                           nstepmax, zinit_fac, gr)
+                           nstepmax, zinit_fac, gr, 1 if solver == "diffeq" else 0)
 
     def dlinear_ab(self, a: float):
         d, h = C.c_double(), C.c_double()
@@ -74,7 +80,7 @@ class EllipsoidOracle:
         return _lib().or_dfnofa(C.byref(self.s.growth), a)
 
     def evolve(self, Frho: float, e_v: float, p_v: float, idynax: int = 1):
-        """(zvir, D, Frho D, steps) of evolve_ellipse_full(..., solver = :rk4)."""
+        """(zvir, D, Frho D, steps) of evolve_ellipse_full with this oracle's solver."""
         out = (C.c_double * 3)()
         n = _lib().or_evolve_ellipse(C.byref(self.s), Frho, e_v, p_v, idynax, out)
         return out[0], out[1], out[2], n

@@ -121,6 +121,7 @@ typedef struct {
     int nstepmax;
     double zinit_fac;
     or_growth growth;
+    int solver;               /* 0: the fixed-step RK4 (:rk4); 1: adaptive Tsit5 (:diffeq) */
 } or_ellipsoid;
 
 void   or_dlinear_ab(const or_growth* g, double ai, double* dlin, double* hd_ha);
@@ -129,6 +130,7 @@ double or_elliptic_rd(double x, double y, double z);
 void   or_get_b_2(double a1, double a2, double a3, double b[3]);
 int    or_evolve_ellipse(const or_ellipsoid* ep, double Frho, double e_v, double p_v,
                          int idynax, double out[3]);
+double or_pow_pos(double x, double y);
 void   or_make_table(const or_ellipsoid* ep, int nx, int ny, int nz, double X1, double X2,
                      double Y1, double Y2, double Z1, double Z2, float* table);
 

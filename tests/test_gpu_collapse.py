@@ -1,11 +1,11 @@
 """GPU parity of the collapse-table generator (ht_evolve_ellipses, ht_collapse_table) with
-the oracle's C restatement of the reference's RK4 ellipsoid collapse
-(EllipsoidalCollapse.jl:149-590) and table sweep (CollapseTable.jl:22-76).
+the oracle's C restatement of the reference's ellipsoid collapse, both integrators: the
+fixed-step RK4 (EllipsoidalCollapse.jl:149-590, solver = :rk4) and the adaptive Tsit5
+(:333-485, solver = :diffeq), and of the table sweep (CollapseTable.jl:22-76).
 
 Both sides run the same FP64 operations in the same order (the device file is built
-without fused multiply-adds), so the values agree to the bit; the one library function on
-the path, log in the oblate branch of the shape integrals, may differ by an ulp, which can
-move an event by at most one RK4 step (a few 1e-3 relative)."""
+without fused multiply-adds, and the logarithm of the oblate shape branch and the Tsit5
+controller's power are series that both carry), so the values agree to the bit."""
 import numpy as np
 import pytest
 import torch
@@ -38,7 +38,7 @@ def _compare(got, want, max_flip=0, step_rel=5e-3, exact_frac=0.99):
 def test_default_table_matches_oracle(ht, planck):
     cp, g = planck
     col = ht.collapse
-    got = col.make_table(col.EllipsoidParams(cp, dlin_tables=g))     # (nz, ny, nx)
+    got = col.make_table(col.EllipsoidParams(cp, dlin_tables=g, solver="rk4"))  # (nz, ny, nx)
     want = np.transpose(oc.EllipsoidOracle(g, cp.Om, cp.OL).make_table(), (2, 1, 0))
     assert got.shape == want.shape == (20, 20, 50) and got.dtype == np.float32
     _compare(got, want)
@@ -54,7 +54,7 @@ def test_evolve_matches_oracle_every_event(ht, planck):
     e = rng.uniform(0.0, 0.5, n)
     p = rng.uniform(-1.0, 1.0, n) * e
     F[:3], e[:3], p[:3] = (1.686, 5.0, 0.5), (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
-    ep = col.EllipsoidParams(cp, dlin_tables=g)
+    ep = col.EllipsoidParams(cp, dlin_tables=g, solver="rk4")
     eo = oc.EllipsoidOracle(g, cp.Om, cp.OL)
     for idynax in (1, 2, 3, 4, 5, 6):
         z, D, fc, st = (t.cpu().numpy() for t in
@@ -76,11 +76,14 @@ def test_other_strategies_match_oracle(ht, planck, fs, vs):
     F = 10.0 ** rng.uniform(np.log10(1.5), np.log10(8.0), n)
     e = rng.uniform(0.0, 0.5, n)
     p = rng.uniform(-1.0, 1.0, n) * e
-    ep = col.EllipsoidParams(cp, iforce_strat=fs, ivir_strat=vs, nstepmax=4000, dlin_tables=g)
-    eo = oc.EllipsoidOracle(g, cp.Om, cp.OL, iforce_strat=fs, ivir_strat=vs, nstepmax=4000)
-    z = col.evolve_ellipses(F, e, p, ep)[0].cpu().numpy()
-    want = np.array([eo.evolve(F[q], e[q], p[q])[0] for q in range(n)])
-    _compare(z, want)
+    for solver in ("rk4", "diffeq"):
+        ep = col.EllipsoidParams(cp, iforce_strat=fs, ivir_strat=vs, nstepmax=4000,
+                                 dlin_tables=g, solver=solver)
+        eo = oc.EllipsoidOracle(g, cp.Om, cp.OL, iforce_strat=fs, ivir_strat=vs,
+                                nstepmax=4000, solver=solver)
+        z = col.evolve_ellipses(F, e, p, ep)[0].cpu().numpy()
+        want = np.array([eo.evolve(F[q], e[q], p[q])[0] for q in range(n)])
+        _compare(z, want)
 
 
 def test_invalid_parameters(ht, planck):
@@ -93,6 +96,8 @@ def test_invalid_parameters(ht, planck):
     ep = col.EllipsoidParams(cp, dlin_tables=g)
     with pytest.raises(ht.HTError):
         col.evolve_ellipses([2.0], [0.1], [0.0], ep, idynax=7)
+    with pytest.raises(ht.HTError):   # the :diffeq path keeps no turnaround events
+        col.evolve_ellipses([2.0], [0.1], [0.0], ep, idynax=4)
     z, D, fc = col.evolve_ellipses(np.zeros(0), np.zeros(0), np.zeros(0), ep)
     assert z.numel() == 0
     with pytest.raises(ht.HTError):
@@ -105,7 +110,7 @@ def test_generated_table_drives_the_finder(ht, planck, tmp_path):
     cp, g = planck
     col = ht.collapse
     path = str(tmp_path / "HomelTab.dat")
-    t = col.generate_table(path, Om=cp.Om, OB=cp.OB, OL=cp.OL, h=cp.h)
+    t = col.generate_table(path, Om=cp.Om, OB=cp.OB, OL=cp.OL, h=cp.h, solver="rk4")
     tab, axes = ht.read_homeltab(path)
     assert np.array_equal(tab, t)
     f = ht.HaloFinder(4, tab, *axes)
@@ -113,3 +118,33 @@ def test_generated_table_drives_the_finder(ht, planck, tmp_path):
     f2 = ht.HaloFinder(4, np.ascontiguousarray(want), *axes)
     assert f.fsc_of_z(0.0) == pytest.approx(f2.fsc_of_z(0.0), rel=1e-6)
     assert 1.6 < f.fsc_of_z(0.0) < 1.8
+
+
+def test_tsit5_table_and_events_match_oracle(ht, planck):
+    """The :diffeq path (adaptive Tsit5) on the device against the oracle's: the default
+    table (the reference's default solver) and events 1-3 of random ellipsoids, with the
+    iterations taken."""
+    cp, g = planck
+    col = ht.collapse
+    got = col.make_table(col.EllipsoidParams(cp, dlin_tables=g))     # solver = "diffeq"
+    want = np.transpose(oc.EllipsoidOracle(g, cp.Om, cp.OL, solver="diffeq").make_table(),
+                        (2, 1, 0))
+    print(f"\nTsit5 table: {np.mean(got == want):.4f} of the entries bit-identical")
+    _compare(got, want, step_rel=0.2)
+    assert (got > 0).sum() > 16900
+    rng = np.random.default_rng(4)
+    n = 400
+    F = 10.0 ** rng.uniform(np.log10(1.2), np.log10(9.0), n)
+    e = rng.uniform(0.0, 0.5, n)
+    p = rng.uniform(-1.0, 1.0, n) * e
+    F[:2], e[:2], p[:2] = (1.686, 0.5), (0.0, 0.0), (0.0, 0.0)
+    ep = col.EllipsoidParams(cp, dlin_tables=g)
+    eo = oc.EllipsoidOracle(g, cp.Om, cp.OL, solver="diffeq")
+    for idynax in (1, 2, 3):
+        z, D, fc, st = (t.cpu().numpy() for t in
+                        col.evolve_ellipses(F, e, p, ep, idynax=idynax, steps=True))
+        want = np.array([eo.evolve(F[q], e[q], p[q], idynax) for q in range(n)])
+        _compare(z, want[:, 0], step_rel=0.2)
+        _compare(D, want[:, 1], step_rel=0.2)
+        assert np.mean(st == want[:, 3]) >= 0.99
+    assert col.evolve_ellipse_full(0.5, 0.0, 0.0, ep) == (-1.0, -1.0, -1.0)
