@@ -219,7 +219,7 @@ static void free_ctx(ht_ctx* c) {
     if (c->tp_n) cufftDestroy(c->tp_plan_n);
     if (c->tp_zc) { cufftDestroy(c->tp_plan_y); cufftDestroy(c->tp_plan_x); }
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
-                    c->d_wrow, c->d_wm1, c->d_wwt, c->d_irad, c->d_irad3, c->d_cell,
+                    c->d_wrow, c->d_wpk, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
                     c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_ftw, c->d_queue,
                     c->d_stats, c->d_chi, c->d_zchi, c->d_atab, c->d_Da, c->d_dlnD,
@@ -274,6 +274,8 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
     for (size_t m = 0; m < rad.size(); ++m)
         if (rad[m] > 0.0) { irad[m] = 1.0 / rad[m]; irad3[m] = 1.0 / (rad[m] * rad[m] * rad[m]); }
     c->nweights = (int64_t)wm1.size();
+    std::vector<double2> wpk(wm1.size());
+    for (size_t e = 0; e < wm1.size(); ++e) wpk[e] = make_double2(wwt[e], (double)wm1[e]);
     int rc;
     if ((rc = upload(&c->d_off, c->h_off.data(), c->h_off.size(), "shell offsets")) ||
         (rc = upload(&c->d_start, c->h_start.data(), c->h_start.size(), "shell starts")) ||
@@ -285,8 +287,7 @@ extern "C" int ht_ctx_create(int device, int nhunt, const float* ct_table_host, 
         (rc = upload(&c->d_ct, c->h_ct.data(), c->h_ct.size(), "collapse table")) ||
         (rc = upload(&c->d_akk, akk.data(), akk.size(), "SPH table")) ||
         (rc = upload(&c->d_wrow, wrow.data(), wrow.size(), "weight rows")) ||
-        (rc = upload(&c->d_wm1, wm1.data(), wm1.size(), "weight shells")) ||
-        (rc = upload(&c->d_wwt, wwt.data(), wwt.size(), "weights")) ||
+        (rc = upload(&c->d_wpk, wpk.data(), wpk.size(), "weights")) ||
         (rc = ht_alloc((void**)&c->d_queue, 256, "work queue")) ||
         (rc = ht_alloc((void**)&c->d_stats, 256, "launch stats"))) {
         free_ctx(c);

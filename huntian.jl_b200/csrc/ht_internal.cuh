@@ -39,8 +39,7 @@ struct ht_ctx {
     // the two shell radii: row mp holds entries [wrow[mp], wrow[mp+1]) of (m1, weight)
     int64_t nweights = 0;
     int32_t* d_wrow = nullptr;     // [nshells + 2]
-    int32_t* d_wm1 = nullptr;
-    double* d_wwt = nullptr;
+    double2* d_wpk = nullptr;      // per entry: (weight, m1 as a double), one 16-byte load
     // result-neutral tunables (ht_ctx_tune)
     int tune_block_bits = 17;      // LEARNED order: spatial block of 2^bits cells
     int tune_pf_kz = 0;            // peak scan: planes per CTA (0: by grid size)

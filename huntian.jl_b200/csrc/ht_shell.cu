@@ -39,14 +39,18 @@ constexpr int kRec = 16;          // doubles per shell in the scratch profile
 constexpr int kSmallG = 8;        // lanes per peak
 constexpr int kPeaksPerItem = 32 / kSmallG;  // peaks per work item (one per group)
 
-// Scratch profile record, one per shell m (1-based):
+// Scratch profile record, one per shell m (1-based); rows are 128-byte aligned, and the
+// twelve values the SPH window sums read (G, Gf, SR) fill the last 96 bytes, so that they
+// come in three 256-bit loads:
 enum : int {
     P_FBAR = 0,
-    P_G = 1,      // 3: Gshell / rad
-    P_GF = 4,     // 3: Gshellf / rad
-    P_SR = 7,     // 6: (SR_LK + SR_KL) / rad for 11, 22, 33, 12, 13, 23
-    P_CSRB = 13,  // running Srb numerator, RadialShell.jl:760-764
+    P_CSRB = 1,   // running Srb numerator, RadialShell.jl:760-764
+    P_G = 4,      // 3: Gshell / rad
+    P_GF = 7,     // 3: Gshellf / rad
+    P_SR = 10,    // 6: (SR_LK + SR_KL) / rad for 11, 22, 33, 12, 13, 23
 };
+static_assert(P_GF == P_G + 3 && P_SR == P_G + 6 && P_SR + 6 == kRec && P_G % 4 == 0,
+              "G, Gf, SR: twelve contiguous doubles on a 32-byte boundary at the row's end");
 
 // Per-cell sums gathered for every shell.
 enum : int { V_F = 0, V_N = 1, V_G = 2, V_GF = 5, V_SR = 8, V_ROWS = 14 };
@@ -83,8 +87,7 @@ struct WalkArgs {
     const double* irad3;    // 1 / rad^3
     int nshells;
     const int32_t* wrow;   // SPH weight table: row mp = entries [wrow[mp], wrow[mp+1])
-    const int32_t* wm1;
-    const double* wwt;
+    const double2* wpk;    // entry: (weight, m1)
 
     const float* ct;
     int nx, ny, nz;
@@ -194,9 +197,21 @@ struct Strain {
 // row of mp = 1 lists shells 2..U(1) with the atab4 weight 0.5 * W / rad[m1].  The
 // weighted sums are scaled by wRnor / rad[mp] (mp > 1) or aRnor (mp = 1) at the end, in
 // the reference's order.
+// The twelve window values (G, Gf, SR) of a profile row in three 256-bit loads.  The rows
+// were written by the group's lanes before the post-processing began (the group synced
+// since), and this is the only access to them in the caller's loop.
+__device__ __forceinline__ void load_row12(const double* q, double (&r)[12]) {
+    const double* b = q + P_G;
+    asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(r[0]), "=d"(r[1]), "=d"(r[2]), "=d"(r[3]) : "l"(b));
+    asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(r[4]), "=d"(r[5]), "=d"(r[6]), "=d"(r[7]) : "l"(b + 4));
+    asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+                 : "=d"(r[8]), "=d"(r[9]), "=d"(r[10]), "=d"(r[11]) : "l"(b + 8));
+}
+
 __device__ __noinline__ Strain kernel_strain(const int32_t* __restrict__ wrow,
-                                             const int32_t* __restrict__ wm1,
-                                             const double* __restrict__ wwt,
+                                             const double2* __restrict__ wpk,
                                              const double* __restrict__ rad, double wRnor,
                                              double aRnor, const double* __restrict__ P,
                                              int mp, int lo, int hi) {
@@ -207,19 +222,21 @@ __device__ __noinline__ Strain kernel_strain(const int32_t* __restrict__ wrow,
     for (int i = 0; i < 3; ++i) { s.g[i] = 0.0; s.gf[i] = 0.0; }
     const int e0 = __ldg(wrow + mp), e1 = __ldg(wrow + mp + 1);
     for (int e = e0; e < e1; ++e) {
-        const int m1 = __ldg(wm1 + e);
+        const double2 we = __ldg(wpk + e);
+        const int m1 = (int)we.y;
         if (m1 > hi) break;
         if (m1 < lo) continue;
-        const double wt = __ldg(wwt + e);
+        const double wt = we.x;
         const double hw = 0.5 * wt;
-        const double* q = P + (size_t)m1 * kRec;
+        double r[12];
+        load_row12(P + (size_t)m1 * kRec, r);
 #pragma unroll
         for (int L = 0; L < 3; ++L) {
-            s.g[L] += wt * q[P_G + L];
-            s.gf[L] += wt * q[P_GF + L];
+            s.g[L] += wt * r[L];
+            s.gf[L] += wt * r[3 + L];
         }
 #pragma unroll
-        for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
+        for (int i = 0; i < 6; ++i) s.E[i] -= hw * r[6 + i];
     }
     const double scale = mp > 1 ? wRnor / rad[mp] : aRnor;
 #pragma unroll
@@ -252,14 +269,15 @@ __device__ __noinline__ Strain kernel_strain_central(const double* __restrict__ 
         if (icon >= 0 && icon < 1100) aww = akk[icon] + diff * (akk[icon + 1] - akk[icon]);
         const double wt = 0.5 * aww / r1;
         const double hw = 0.5 * wt;
-        const double* q = P + (size_t)m1 * kRec;
+        double r[12];
+        load_row12(P + (size_t)m1 * kRec, r);
 #pragma unroll
         for (int L = 0; L < 3; ++L) {
-            s.g[L] += wt * q[P_G + L];
-            s.gf[L] += wt * q[P_GF + L];
+            s.g[L] += wt * r[L];
+            s.gf[L] += wt * r[3 + L];
         }
 #pragma unroll
-        for (int i = 0; i < 6; ++i) s.E[i] -= hw * q[P_SR + i];
+        for (int i = 0; i < 6; ++i) s.E[i] -= hw * r[6 + i];
     }
 #pragma unroll
     for (int i = 0; i < 6; ++i) s.E[i] *= aRnor;
@@ -274,7 +292,7 @@ __device__ __noinline__ Strain kernel_strain_central(const double* __restrict__ 
 // local memory and read its fields from there.)
 __device__ __forceinline__ Strain strain_at(const WalkArgs& a, const double* P, int mp,
                                             int lo, int hi) {
-    return kernel_strain(a.wrow, a.wm1, a.wwt, a.rad, a.wRnor, a.aRnor, P, mp, lo, hi);
+    return kernel_strain(a.wrow, a.wpk, a.rad, a.wRnor, a.aRnor, P, mp, lo, hi);
 }
 __device__ __forceinline__ Strain strain_central(const WalkArgs& a, const double* P, int lo,
                                                  int hi) {
@@ -691,10 +709,11 @@ __device__ __forceinline__ void process_peak(const WalkArgs& a, long long p, dou
         csrb += 0.5 * (Fbarp + Fbar_s) * (r5 - rad5p);
         double* q = P + (size_t)s * kRec;
         if (!HT_INDEX_OK(a.status, s, a.nshells + 2)) break;
-        for (int i = t; i <= P_CSRB; i += G) {
+        for (int i = t; i < kRec; i += G) {
             double v;
             if (i == P_FBAR) v = Fbar_s;
             else if (i == P_CSRB) v = csrb;
+            else if (i < P_G) continue;   // unused
             else if (i >= P_SR && i < P_SR + 3) v = (2.0 * R[(V_G + i - P_G) * RP + G]) * a.irad[s];
             else v = R[(V_G + i - P_G) * RP + G] * a.irad[s];   // G, Gf, SR rows in order
             q[i] = v;
@@ -1205,7 +1224,7 @@ static void fill_args(WalkArgs& a, const ht_ctx* ctx, const ht_fields& f, const 
     a.irad = ctx->d_irad; a.irad3 = ctx->d_irad3;
     a.cell = nullptr; a.nhunt = ctx->nhunt;
     for (int jj = 0; jj < 10; ++jj) a.zh_frac[jj] = cbrt(jj / 9.0 * 0.5 + 0.5);
-    a.wrow = ctx->d_wrow; a.wm1 = ctx->d_wm1; a.wwt = ctx->d_wwt;
+    a.wrow = ctx->d_wrow; a.wpk = ctx->d_wpk;
     a.ct = ctx->d_ct; a.nx = ctx->nx; a.ny = ctx->ny; a.nz = ctx->nz;
     a.X1 = ctx->X1; a.X2 = ctx->X2; a.Y1 = ctx->Y1; a.Y2 = ctx->Y2; a.Z1 = ctx->Z1;
     a.Z2 = ctx->Z2; a.out_val = ctx->out_val; a.akk = ctx->d_akk;
