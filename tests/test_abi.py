@@ -32,6 +32,18 @@ def test_library_exports_every_declared_symbol(ht):
     assert exported == _declared()
 
 
+def test_checked_library_exports_the_same_symbols(ht):
+    """libhuntian_b200_checked.so (build.py --checked, -DHT_CHECKED) is the same C ABI:
+    every declared entry point and nothing else."""
+    path = os.path.join(os.path.dirname(ht.LIB_PATH), "libhuntian_b200_checked.so")
+    if not os.path.exists(path):
+        pytest.skip("checked build not present (python huntian.jl_b200/build.py --checked)")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True,
+                         text=True, check=True).stdout
+    exported = sorted(ln.split()[-1] for ln in out.splitlines() if " T " in ln)
+    assert exported == _declared()
+
+
 def test_errors_are_status_codes(ht):
     lib = ht._lib.load()
     h = C.c_void_p()
