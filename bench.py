@@ -481,8 +481,14 @@ def run_ours(args, rank, world, device):
     ms_per_step = t_ms / args.steps
     value = tot_peaks / (t_ms / 1e3)
 
-    # e2e through the public mirror with host buffers (rank 0 measures, all ranks run)
+    # e2e through the public mirror with host buffers: every rank runs its own tile's
+    # pipeline; the whole job's rate is the peaks of all ranks over the slowest rank's time,
+    # and the copied bytes are summed over the ranks
+    if dist:
+        torch.distributed.barrier()
     e2e = run_e2e(ht, W, args) if args.e2e_steps > 0 else None
+    if dist and e2e is not None:
+        e2e = ht.dist.aggregate_e2e(e2e)
 
     if rank != 0:
         return None

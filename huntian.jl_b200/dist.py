@@ -128,6 +128,26 @@ def sum_over_ranks(value: float, group=None) -> float:
     return float(t.item())
 
 
+def aggregate_e2e(e2e: dict, group=None) -> dict:
+    """The whole job's end-to-end line from every rank's own (value = units per second over
+    `steps` steps of `ms_per_step`, bytes copied per step): the units of all ranks over the
+    slowest rank's time, the copied bytes summed over ranks.  Every rank calls it (it holds
+    collectives); without an initialised process group it returns the line unchanged."""
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        return dict(e2e)
+    out = dict(e2e)
+    steps = e2e["steps"]
+    units = e2e["value"] * e2e["ms_per_step"] * steps / 1e3
+    ms = max_over_ranks(e2e["ms_per_step"], group)
+    out["ms_per_step"] = ms
+    out["value"] = sum_over_ranks(units, group) / (ms * steps / 1e3)
+    out["h2d_bytes_per_step"] = int(sum_over_ranks(e2e["h2d_bytes_per_step"], group))
+    out["d2h_bytes_per_step"] = int(sum_over_ranks(e2e["d2h_bytes_per_step"], group))
+    out["ranks"] = dist.get_world_size(group)
+    return out
+
+
 def merge_catalog(parts: Sequence[np.ndarray]) -> np.ndarray:
     """Rank-order concatenation of per-rank records (halo order across workers carries no
     meaning, MultiResolution.jl:1338)."""

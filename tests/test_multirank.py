@@ -1,6 +1,6 @@
 """Multi-rank host logic on CPU (gloo, world size 2): tile sharding, peak-range splits, the
-end-of-run catalog gather (MPIExt.jl:1041-1063 mirror), max-over-ranks timing, and a rank
-that leaves before the gather.  The per-rank compute is the CPU oracle standing in for the
+end-of-run catalog gather (MPIExt.jl:1041-1063 mirror), max-over-ranks timing, the bench's
+whole-job end-to-end aggregate, and a rank that leaves before the gather.  The per-rank compute is the CPU oracle standing in for the
 device collapse, so the test checks the plumbing: a catalog split over ranks and gathered
 equals the one-rank catalog record for record."""
 import os
@@ -166,6 +166,38 @@ def test_split_catalog_equals_single_rank(ht):
     np.testing.assert_array_equal(got, whole)
     assert out[0][2] == out[1][2] == 11.0
     assert out[0][3] == out[1][3] == float(len(pi))
+
+
+def _worker_e2e(rank, port, q):
+    try:
+        dist = _init(rank, port)
+        ht = load_package()
+        # rank r: 100 (r + 1) units per step over 4 steps of 10 (r + 1) ms
+        mine = {"value": 100.0 * (rank + 1) / (10.0 * (rank + 1) / 1e3), "unit": "u/s",
+                "ms_per_step": 10.0 * (rank + 1), "steps": 4,
+                "h2d_bytes_per_step": 1000 * (rank + 1), "d2h_bytes_per_step": 7}
+        got = ht.dist.aggregate_e2e(mine)
+        q.put((rank, got, None, None, None))
+        dist.barrier()
+        dist.destroy_process_group()
+    except Exception as e:
+        q.put((rank, "ERR " + repr(e), None, None, None))
+
+
+def test_e2e_aggregates_over_ranks(ht):
+    """The bench's whole-job end-to-end line at N ranks: all ranks' units over the slowest
+    rank's time, the copied bytes summed (and the one-rank line unchanged)."""
+    one = {"value": 5.0, "ms_per_step": 2.0, "steps": 3, "h2d_bytes_per_step": 1,
+           "d2h_bytes_per_step": 2}
+    assert ht.dist.aggregate_e2e(one) == one
+    out, codes = _run(_worker_e2e)
+    assert codes == [0] * WORLD, out
+    for r in range(WORLD):
+        got = out[r][1]
+        assert not isinstance(got, str), got
+        assert got["ms_per_step"] == 20.0 and got["ranks"] == WORLD
+        assert abs(got["value"] - (100.0 + 200.0) / 0.020) < 1e-9
+        assert got["h2d_bytes_per_step"] == 3000 and got["d2h_bytes_per_step"] == 14
 
 
 def _worker_leaves(rank, port, q):
