@@ -12,8 +12,8 @@
 // soon as every shell the post-processing reads has been gathered.  The same group then
 // runs the post-processing of RadialShell.jl:449-859 / ext/CUDAExt.jl:1213-1912 in FP64:
 // fcrit crossing, the inward strain/eigen/barrier walk (G steps evaluated at once, one per
-// lane), RTHL interpolation, Sbar (a second pass over the cells within the collapsed
-// radius), Srb, d2F, zvir_half and the mask update.  The SPH window weights of
+// lane), RTHL interpolation, Sbar and the mask update (one second pass over the cells within
+// the collapsed radius), Srb, d2F and zvir_half.  The SPH window weights of
 // kernel_strain depend only on the two shell radii, so they come from a table built once
 // per context.
 //
