@@ -451,6 +451,7 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(device.index or 0) if rank == 0 else None
+    W.finder.reset_reject_counts()          # stream-ordered, before the timed steps
     nf = len(W.filters)
     mk = lambda: torch.cuda.Event(enable_timing=True)
     evs = [{"pf": [(mk(), mk()) for _ in range(nf)], "pack": (mk(), mk()),
@@ -466,6 +467,7 @@ def run_ours(args, rank, world, device):
         torch.distributed.barrier()
     torch.cuda.synchronize()
     ck = clocks.stop() if clocks else None
+    rejects = {k: v // args.steps for k, v in W.finder.reject_counts().items()}
     t_ms = start.elapsed_time(end)
     npf = nf if W.graph is None else 1    # with the graph one event pair spans the loop
     pf_ms = sum(a.elapsed_time(b) for e in evs for a, b in e["pf"][:npf]) / args.steps
@@ -529,6 +531,9 @@ def run_ours(args, rank, world, device):
         "clocks": ck,
         "e2e": e2e,
     }
+    # why the timed steps' peaks ended without collapse (the reference's counters,
+    # RadialShell.jl:13-32, kept on the device), per step
+    line["reject_counts_per_step"] = rejects
     line["post_step_ms"] = post_step(ht, W)
     line["walk_modes"] = W.walk_modes() if args.compare_modes else None
     # the walk's second ceiling: scattered 32-byte gathers with no reuse, measured here
