@@ -98,7 +98,33 @@ __global__ void __launch_bounds__(256) features_kernel(const FeatArgs a, float* 
     };
     float v;
     if (value(ci, cj, ck, v)) f[5] = v;
-    for (int s = 2; s <= 5 && s <= a.nshells; ++s) {
+    // shells 2-5 (r^2 = 1, 2, 3, 4) hold 6, 12, 8 and 6 cells, the table's first 32 after the
+    // centre: a peak at least two cells inside the tile has every one of them, so all 32
+    // loads go out before any is summed (same sums, same order as the loop below)
+    const bool inner2 = a.nshells >= 5 && ci > 2 && ci + 2 <= a.n1 && cj > 2 &&
+                        cj + 2 <= a.n2 && ck > 2 && ck + 2 <= a.n3;
+    if (inner2) {
+        const long long c0 = (long long)(ci - 1) + (long long)a.n1 * (cj - 1) + a.s2 * (ck - 1);
+        const int st2 = __ldg(a.start + 2);
+        float w[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            const char4 o = __ldg(a.off + st2 + c);
+            const long long idx = c0 + o.x + (long long)a.n1 * o.y + a.s2 * o.z;
+            w[c] = a.rec ? __ldg(reinterpret_cast<const float*>(a.rec + 2 * idx))
+                         : __ldg(a.delta + idx);
+        }
+        constexpr int kFirst[5] = {0, 6, 18, 26, 32};
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            float sum = 0.f;
+#pragma unroll
+            for (int c = kFirst[s]; c < kFirst[s + 1]; ++c) sum += w[c];
+            const int nin = kFirst[s + 1] - kFirst[s];
+            f[6 + s] = sum / nin;
+        }
+    }
+    for (int s = 2; !inner2 && s <= 5 && s <= a.nshells; ++s) {
         const int st = __ldg(a.start + s), cnt = __ldg(a.count + s);
         float sum = 0.f;
         int nin = 0;

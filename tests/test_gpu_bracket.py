@@ -172,3 +172,50 @@ def test_shipped_weights_predict_walks(ht, oracle, julia_table_path):
     P = br.predict(finder, model, F).cpu().numpy()
     assert np.isfinite(P).all()
     assert F.shape == (npk, 16)
+
+
+def test_features_match_numpy(ht, finder):
+    """The per-peak features (ht_bracket_features) against a numpy restatement, for peaks
+    inside the tile (all 32 cells of the shells r^2 = 1..4 present: the unrolled path) and
+    on its faces, edges and corners (out-of-tile cells left out of the shell means)."""
+    br = ht.bracket
+    rng = np.random.default_rng(21)
+    n = 20
+    d = rng.standard_normal((n, n, n)).astype(np.float32)      # [k][j][i], i fastest
+    eta = [rng.standard_normal((n, n, n)).astype(np.float32) for _ in range(3)]
+    dev = lambda a, dt=torch.float32: torch.as_tensor(np.ascontiguousarray(a), dtype=dt,
+                                                       device="cuda")
+    finder.bind_fields(dev(d), *[dev(e) for e in eta])
+    pts = [(i, j, k) for i in (1, 2, 3, 10, n - 1, n) for j in (1, 3, 11, n)
+           for k in (1, 2, 9, n - 2, n)]
+    pts += [tuple(int(x) for x in rng.integers(1, n + 1, 3)) for _ in range(200)]
+    pi, pj, pk = (np.array([p[a] for p in pts], np.int32) for a in range(3))
+    npk = len(pts)
+    Rf = rng.uniform(1.5, 6.0, npk)
+    ir2 = rng.integers(1, 30, npk).astype(np.int32)
+    zz = rng.uniform(1.0, 2.0, npk).astype(np.float32)
+    fc = rng.uniform(1.5, 1.8, npk).astype(np.float32)
+    pd = rng.standard_normal(npk).astype(np.float32)
+    alatt = 1.3
+    F = br.features(finder, dev(pi, torch.int32), dev(pj, torch.int32), dev(pk, torch.int32),
+                    dev(Rf, torch.float64), dev(ir2, torch.int32), dev(zz), dev(fc), alatt,
+                    peak_delta=dev(pd)).cpu().numpy()
+    r2 = finder.shell_r2().astype(np.int64)          # entry m - 1 is shell m
+    ns = len(r2)
+    offs = {s: [(a, b, c) for c in range(-2, 3) for b in range(-2, 3) for a in range(-2, 3)
+                if a * a + b * b + c * c == s] for s in (1, 2, 3, 4)}
+    want = np.zeros((npk, 16), np.float32)
+    for q, (i, j, k) in enumerate(pts):
+        want[q, 0] = Rf[q] / alatt
+        want[q, 1] = np.sqrt(np.float32(ir2[q]))
+        want[q, 2], want[q, 3], want[q, 4] = pd[q], fc[q], zz[q]
+        want[q, 5] = d[k - 1, j - 1, i - 1]
+        for s in (1, 2, 3, 4):
+            v = [d[k - 1 + c, j - 1 + b, i - 1 + a] for a, b, c in offs[s]
+                 if 1 <= i + a <= n and 1 <= j + b <= n and 1 <= k + c <= n]
+            want[q, 5 + s] = np.sum(np.float64(v)) / len(v) if v else 0.0
+        m0 = next((m for m in range(1, ns) if r2[m - 1] > ir2[q]), ns - 1)
+        want[q, 10] = np.sqrt(float(r2[m0 - 1]))
+        want[q, 11] = Rf[q] / alatt + 2.0
+    np.testing.assert_allclose(F[:, :12], want[:, :12], rtol=2e-6, atol=2e-6)
+    assert np.all(F[:, 12:] == 0)
