@@ -1,5 +1,5 @@
 // Learned walk-length bracket: a 12 -> 64 -> 64 -> 64 -> 2 MLP (BF16 weights and
-// activations, FP32 accumulation on the tensor cores with mma.sync m16n8k16) that predicts,
+// activations, FP32 accumulation on the tensor cores) that predicts,
 // for every peak, a low and a high quantile of the radius at which its shell walk stops.
 // The shell collapse itself never reads the prediction: it only orders the work (peaks with
 // similar predicted walks share a warp, longest first), so every result is identical to the
@@ -16,10 +16,11 @@
 //
 // Kernels:
 //   features_kernel      one thread per peak
-//   mlp_infer_kernel     one warp per 16 peaks: the four layers chained in registers (the
-//                        FP32 accumulator fragment of a layer, after bias and ReLU, is
-//                        repacked as the BF16 A fragment of the next)
-//   gemm_bf16_kernel     generic C = op(A) op(B) (BF16 in, FP32 out) for training:
+//   mlp_infer_tc_kernel  inference, 128 peaks per CTA tile: every layer a tcgen05.mma chain
+//                        from shared memory into tensor memory, read back per row
+//                        (tcgen05.ld), bias + ReLU + BF16 as the next layer's operand
+//   gemm_bf16_kernel     generic C = op(A) op(B) (BF16 in, FP32 out, mma.sync m16n8k16)
+//                        for training (offline, not on the step):
 //                        forward products, activation gradients and weight gradients
 //   small elementwise kernels for bias/ReLU, the pinball-loss gradient, ReLU backward,
 //   bias gradients and Adam.
@@ -29,6 +30,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <string>
 
+#include "ht_async.cuh"
 #include "ht_internal.cuh"
 
 namespace {
@@ -164,78 +166,248 @@ struct MlpW {
     const float* istd;         // [16]
 };
 
-// B fragment (k = 2 tig .. 2 tig + 1 and + 8, n = group) of row-major W[n][k] with row
-// stride K, for the n-tile starting at n0 and the k-slice starting at k0.
-__device__ __forceinline__ void load_b(const __nv_bfloat16* W, int K, int n0, int k0,
-                                       int lane, unsigned& b0, unsigned& b1) {
-    const int g = lane >> 2, t = lane & 3;
-    const unsigned* row = reinterpret_cast<const unsigned*>(W + (size_t)(n0 + g) * K + k0);
-    b0 = __ldg(row + t);
-    b1 = __ldg(row + t + 4);
+// ------------------------------------------------- fused inference, tcgen05 ----
+//
+// The same four layers on the 5th-generation tensor cores.  A CTA of 128 threads takes
+// tiles of 128 peaks (M = 128), persistent over the tiles.  Every layer is a chain of
+// tcgen05.mma (kind::f16, BF16 x BF16 -> FP32, one elected thread issues them) from shared
+// memory into a 64-column accumulator in tensor memory: the activations A [128 x K] and the
+// layer's weights W [N x K] (the row-major weights are K-major already) sit in the
+// no-swizzle K-major layout of 8-row x 16-byte core matrices.  The MMAs of a layer are
+// committed to an mbarrier; every thread then reads its own row back (tcgen05.ld 32x32b:
+// warp w owns lanes 32w .. 32w + 31, and row r of an M = 128 accumulator is lane r), adds
+// the bias, applies ReLU, rounds to BF16 and writes the row as the next layer's A.  The
+// output layer is padded to N = 16 (weight rows 2 .. 15 zero).  Waits are bounded; a wait
+// that gives up records the status, and the CTA still frees its tensor memory.
+
+constexpr int kTcRows = 128;    // peaks per tile (the MMA's M)
+constexpr int kTcN4 = 16;       // the output layer's N (2 used)
+constexpr int kTcCols = 64;     // tensor-memory columns per CTA (FP32 accumulator, N <= 64)
+
+// Byte offset of element (r, k) in a K-major operand of R rows: core matrices of 8 rows x
+// 8 K-values (16 bytes a row, 128 bytes each), row groups 128 bytes apart (the descriptor's
+// stride offset), the two K halves of a 16-wide K step R x 16 bytes apart (its leading
+// offset), K steps R x 32 bytes apart.
+__host__ __device__ constexpr int umma_off(int R, int r, int k) {
+    return (k >> 4) * (R * 32) + ((k >> 3) & 1) * (R * 16) + (r >> 3) * 128 + (r & 7) * 16 +
+           (k & 7) * 2;
 }
 
-// Hidden layer: 64 outputs from A fragments covering K (kq slices of 16); bias + ReLU; the
-// result repacked as 4 A fragments (K = 64) for the next layer.
-template <int KQ>
-__device__ __forceinline__ void hidden_layer(const unsigned (&A)[KQ][4],
-                                             const __nv_bfloat16* W, const float* b, int lane,
-                                             unsigned (&Aout)[4][4]) {
-    const int t = lane & 3;
+// Shared-memory matrix descriptor of such an operand (R rows) starting at shared address
+// saddr: start >> 4 in bits [0, 14), leading offset >> 4 in [16, 30), stride offset >> 4
+// in [32, 46), version 1 in [46, 48), no swizzle, base offset 0.
+__device__ __forceinline__ unsigned long long umma_desc(unsigned saddr, int R) {
+    const unsigned long long lbo = (unsigned long long)(R * 16) >> 4, sbo = 128ull >> 4;
+    return (unsigned long long)((saddr >> 4) & 0x3FFFu) | (lbo << 16) | (sbo << 32) |
+           (1ull << 46);
+}
+
+// Instruction descriptor: FP32 accumulator, BF16 A and B, both K-major, N >> 3 in bits
+// [17, 23), M >> 4 in bits [24, 29).
+__host__ __device__ constexpr unsigned umma_idesc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(N >> 3) << 17) |
+           ((unsigned)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(unsigned tmem_d, unsigned long long da,
+                                          unsigned long long db, unsigned idesc,
+                                          unsigned accumulate) {
+    const unsigned z = 0u;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :: "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z),
+           "r"(z));
+}
+
+__device__ __forceinline__ void umma_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 :: "r"(htasync::smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 16 consecutive accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(unsigned taddr, float (&v)[16]) {
+    unsigned u[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(u[0]), "=r"(u[1]), "=r"(u[2]), "=r"(u[3]), "=r"(u[4]), "=r"(u[5]), "=r"(u[6]),
+          "=r"(u[7]), "=r"(u[8]), "=r"(u[9]), "=r"(u[10]), "=r"(u[11]), "=r"(u[12]),
+          "=r"(u[13]), "=r"(u[14]), "=r"(u[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float c[4];
-        const float bb0 = __ldg(b + 8 * j + 2 * t), bb1 = __ldg(b + 8 * j + 2 * t + 1);
-        c[0] = bb0; c[1] = bb1; c[2] = bb0; c[3] = bb1;
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(u[i]);
+}
+
+// Shared-memory layout of the tcgen05 inference kernel (bytes from the dynamic base).
+constexpr int kTcOffA = 0;                                  // A [128 x 64] BF16
+constexpr int kTcOffW1 = kTcOffA + kTcRows * kHid * 2;      // W1 [64 x 16]
+constexpr int kTcOffW2 = kTcOffW1 + kHid * kIn * 2;         // W2 [64 x 64]
+constexpr int kTcOffW3 = kTcOffW2 + kHid * kHid * 2;        // W3 [64 x 64]
+constexpr int kTcOffW4 = kTcOffW3 + kHid * kHid * 2;        // W4 [16 x 64]
+constexpr int kTcOffB = kTcOffW4 + kTcN4 * kHid * 2;        // b1 b2 b3 [64] b4 [8], FP32
+constexpr int kTcSmem = kTcOffB + (3 * kHid + 8) * 4;
+
+// Copy the row-major weights W [rows x K] (global, BF16) into the K-major layout with Rpad
+// rows (rows >= rows zero).
+__device__ __forceinline__ void stage_weights(unsigned char* dst, const __nv_bfloat16* W,
+                                              int rows, int Rpad, int K, int tid, int nthr) {
+    for (int e = tid; e < Rpad * (K / 2); e += nthr) {
+        const int r = e / (K / 2), k = 2 * (e % (K / 2));
+        const unsigned v = r < rows ? __ldg(reinterpret_cast<const unsigned*>(W + (size_t)r * K + k))
+                                    : 0u;
+        *reinterpret_cast<unsigned*>(dst + umma_off(Rpad, r, k)) = v;
+    }
+}
+
+// Bias, ReLU and BF16 rounding of the 64 columns of this thread's row, written as row r of
+// the next layer's A.
+__device__ __forceinline__ void hidden_out(unsigned tmem_row, const float* bias,
+                                           unsigned char* A, int r) {
 #pragma unroll
-        for (int q = 0; q < KQ; ++q) {
-            unsigned b0, b1;
-            load_b(W, 16 * KQ, 8 * j, 16 * q, lane, b0, b1);
-            mma_bf16(c, A[q], b0, b1);
+    for (int q = 0; q < kHid / 16; ++q) {
+        float v[16];
+        tmem_ld16(tmem_row + 16 * q, v);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            uint4 u;
+            unsigned* pu = reinterpret_cast<unsigned*>(&u);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int c = 8 * h + 2 * j;
+                pu[j] = pack_bf16(fmaxf(v[c] + bias[16 * q + c], 0.f),
+                                  fmaxf(v[c + 1] + bias[16 * q + c + 1], 0.f));
+            }
+            *reinterpret_cast<uint4*>(A + umma_off(kTcRows, r, 16 * q + 8 * h)) = u;
         }
-        const unsigned lo = pack_bf16(fmaxf(c[0], 0.f), fmaxf(c[1], 0.f));
-        const unsigned hi = pack_bf16(fmaxf(c[2], 0.f), fmaxf(c[3], 0.f));
-        // n-tile j holds columns 8j..8j+7 = k-slice j/2, half (j & 1)
-        Aout[j >> 1][(j & 1) * 2 + 0] = lo;
-        Aout[j >> 1][(j & 1) * 2 + 1] = hi;
     }
 }
 
-__global__ void __launch_bounds__(128) mlp_infer_kernel(const MlpW w, const float* __restrict__ F,
-                                                        long long n, float* __restrict__ Y) {
-    const int lane = threadIdx.x & 31;
-    const long long r0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 16;
-    if (r0 >= n) return;
-    const int g = lane >> 2, t = lane & 3;
-    // A fragment of the standardised features: rows r0 + g, r0 + g + 8; cols 2t, 2t+1 and
-    // 2t+8, 2t+9
-    unsigned X[1][4];
-    {
-        const long long ra = r0 + g, rb = r0 + g + 8;
-        auto fv = [&](long long r, int c) {
-            if (r >= n) return 0.f;
-            return (__ldg(F + r * kIn + c) - __ldg(w.mean + c)) * __ldg(w.istd + c);
-        };
-        X[0][0] = pack_bf16(fv(ra, 2 * t), fv(ra, 2 * t + 1));
-        X[0][1] = pack_bf16(fv(rb, 2 * t), fv(rb, 2 * t + 1));
-        X[0][2] = pack_bf16(fv(ra, 2 * t + 8), fv(ra, 2 * t + 9));
-        X[0][3] = pack_bf16(fv(rb, 2 * t + 8), fv(rb, 2 * t + 9));
+__global__ void __launch_bounds__(kTcRows) mlp_infer_tc_kernel(const MlpW w,
+                                                               const float* __restrict__ F,
+                                                               long long n,
+                                                               float* __restrict__ Y,
+                                                               int32_t* status,
+                                                               long long wait_ns) {
+    extern __shared__ __align__(128) unsigned char tsm[];
+    __shared__ __align__(8) unsigned long long bar;
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5;
+    unsigned char* A = tsm + kTcOffA;
+    float* bias = reinterpret_cast<float*>(tsm + kTcOffB);
+    stage_weights(tsm + kTcOffW1, w.W1, kHid, kHid, kIn, tid, kTcRows);
+    stage_weights(tsm + kTcOffW2, w.W2, kHid, kHid, kHid, tid, kTcRows);
+    stage_weights(tsm + kTcOffW3, w.W3, kHid, kHid, kHid, tid, kTcRows);
+    stage_weights(tsm + kTcOffW4, w.W4, 2, kTcN4, kHid, tid, kTcRows);
+    for (int i = tid; i < kHid; i += kTcRows) {
+        bias[i] = __ldg(w.b1 + i);
+        bias[kHid + i] = __ldg(w.b2 + i);
+        bias[2 * kHid + i] = __ldg(w.b3 + i);
     }
-    unsigned H1[4][4], H2[4][4], H3[4][4];
-    hidden_layer<1>(X, w.W1, w.b1, lane, H1);
-    hidden_layer<4>(H1, w.W2, w.b2, lane, H2);
-    hidden_layer<4>(H2, w.W3, w.b3, lane, H3);
-    float c[4];
-    const float bb0 = __ldg(w.b4 + 2 * t), bb1 = __ldg(w.b4 + 2 * t + 1);
-    c[0] = bb0; c[1] = bb1; c[2] = bb0; c[3] = bb1;
+    if (tid < 8) bias[3 * kHid + tid] = __ldg(w.b4 + tid);
+    if (tid == 0) {
+        htasync::bar_init(&bar, 1);
+        htasync::bar_init_fence();
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(htasync::smem_addr(&tmem_slot)), "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    htasync::fence_async_smem();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_slot;
+    const unsigned tmem_row = tmem + ((unsigned)(32 * warp) << 16);   // this warp's lanes
+    const unsigned sA = htasync::smem_addr(A);
+    const unsigned sW1 = htasync::smem_addr(tsm + kTcOffW1), sW2 = htasync::smem_addr(tsm + kTcOffW2),
+                   sW3 = htasync::smem_addr(tsm + kTcOffW3), sW4 = htasync::smem_addr(tsm + kTcOffW4);
+    const float* mean = w.mean;
+    const float* istd = w.istd;
+    const long long ntiles = (n + kTcRows - 1) / kTcRows;
+    unsigned parity = 0;
+    bool ok = true;
+    // one layer: the MMAs over nk K steps, committed; every thread waits for them
+    auto layer = [&](unsigned sB, int RB, int nk, int N) -> bool {
+        htasync::fence_async_smem();   // this thread's A writes, seen by the tensor cores
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const unsigned idesc = umma_idesc(kTcRows, N);
+            for (int s = 0; s < nk; ++s)
+                umma_bf16(tmem, umma_desc(sA + s * (kTcRows * 32), kTcRows),
+                          umma_desc(sB + s * (RB * 32), RB), idesc, s > 0 ? 1u : 0u);
+            umma_commit(&bar);
+        }
+        const bool done = htasync::bar_wait(&bar, parity, wait_ns);
+        parity ^= 1u;
+        tc_fence_after();
+        return !__syncthreads_or(!done);
+    };
+    for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const long long row = tile * kTcRows + tid;
+        {   // layer-1 input: the standardised features of this thread's peak, BF16
+            float x[kIn];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        unsigned b0, b1;
-        load_b(w.W4, kHid, 0, 16 * q, lane, b0, b1);
-        mma_bf16(c, H3[q], b0, b1);
+            for (int c = 0; c < kIn; c += 4) {
+                const float4 f4 = row < n ? __ldg(reinterpret_cast<const float4*>(F + row * kIn + c))
+                                          : make_float4(0.f, 0.f, 0.f, 0.f);
+                x[c] = f4.x; x[c + 1] = f4.y; x[c + 2] = f4.z; x[c + 3] = f4.w;
+            }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint4 u;
+                unsigned* pu = reinterpret_cast<unsigned*>(&u);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int c = 8 * h + 2 * j;
+                    const float a0 = row < n ? (x[c] - __ldg(mean + c)) * __ldg(istd + c) : 0.f;
+                    const float a1 = row < n ? (x[c + 1] - __ldg(mean + c + 1)) * __ldg(istd + c + 1)
+                                             : 0.f;
+                    pu[j] = pack_bf16(a0, a1);
+                }
+                *reinterpret_cast<uint4*>(A + umma_off(kTcRows, tid, 8 * h)) = u;
+            }
+        }
+        if (!(ok = layer(sW1, kHid, 1, kHid))) break;
+        hidden_out(tmem_row, bias, A, tid);
+        if (!(ok = layer(sW2, kHid, kHid / 16, kHid))) break;
+        hidden_out(tmem_row, bias + kHid, A, tid);
+        if (!(ok = layer(sW3, kHid, kHid / 16, kHid))) break;
+        hidden_out(tmem_row, bias + 2 * kHid, A, tid);
+        if (!(ok = layer(sW4, kTcN4, kHid / 16, kTcN4))) break;
+        {
+            unsigned u0, u1;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0, %1}, [%2];"
+                         : "=r"(u0), "=r"(u1) : "r"(tmem_row));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < n) {
+                Y[row * 2] = __uint_as_float(u0) + bias[3 * kHid];
+                Y[row * 2 + 1] = __uint_as_float(u1) + bias[3 * kHid + 1];
+            }
+        }
     }
-    if (t == 0) {   // columns 0 and 1 are the two outputs
-        if (r0 + g < n) { Y[(r0 + g) * 2] = c[0]; Y[(r0 + g) * 2 + 1] = c[1]; }
-        if (r0 + g + 8 < n) { Y[(r0 + g + 8) * 2] = c[2]; Y[(r0 + g + 8) * 2 + 1] = c[3]; }
+    if (!ok && tid == 0) {
+        // record the timeout, then give the MMAs in flight a bounded time to finish
+        atomicExch(status, kStatusWaitTimeout);
+        htasync::bar_wait(&bar, parity ^ 1u, wait_ns);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                     :: "r"(tmem), "r"(kTcCols));
     }
 }
 
@@ -479,11 +651,15 @@ extern "C" HT_API int ht_bracket_predict(ht_ctx* ctx, const ht_bracket_model* m,
     if (rc != HT_OK) return rc;
     if (n < 0) return ht_fail(HT_ERR_INVALID, "ht_bracket_predict: n < 0");
     if (n == 0) return HT_OK;
+    if (((uintptr_t)d_feat & 15u) != 0)
+        return ht_fail(HT_ERR_INVALID, "ht_bracket_predict: d_feat must be 16-byte aligned");
     HT_CUDA_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
-    const long long tiles = (n + 15) / 16;   // 16 peaks per warp, 4 warps per block
-    mlp_infer_kernel<<<blocks_for(tiles, 4), 128, 0, (cudaStream_t)stream>>>(mlp_of(m), d_feat,
-                                                                              n, d_pred);
-    HT_CUDA_TRY(cudaGetLastError(), "mlp_infer_kernel launch");
+    // persistent CTAs of 128 peaks, four per SM (each holds 64 tensor-memory columns)
+    const long long tiles = (n + kTcRows - 1) / kTcRows;
+    const unsigned grid = (unsigned)std::min<long long>(tiles, 4LL * ctx->num_sms);
+    mlp_infer_tc_kernel<<<grid, kTcRows, kTcSmem, (cudaStream_t)stream>>>(
+        mlp_of(m), d_feat, n, d_pred, ht_status_word(ctx), ctx->wait_ns);
+    HT_CUDA_TRY(cudaGetLastError(), "mlp_infer_tc_kernel launch");
     ctx->last_kernels = 1;
     return HT_OK;
 }

@@ -450,7 +450,9 @@ HT_API int ht_bracket_features(ht_ctx* ctx, const ht_peak_batch* batch,
                                void* stream);
 
 /* Inference: d_pred [n x 2] FP32 (low, high quantile of the stop radius, lattice units)
- * from d_feat [n x 16].  Tensor cores (mma.sync BF16, FP32 accumulation). */
+ * from d_feat [n x 16] (16-byte aligned).  5th-generation tensor cores (tcgen05.mma, BF16
+ * operands in shared memory, FP32 accumulators in tensor memory); a bounded wait that gives
+ * up sets ht_device_status to 1. */
 HT_API int ht_bracket_predict(ht_ctx* ctx, const ht_bracket_model* model, const float* d_feat,
                               int64_t n, float* d_pred, void* stream);
 
