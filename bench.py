@@ -541,7 +541,7 @@ def run_ours(args, rank, world, device):
     line["roofline"]["random_gather_ceiling_gbs"] = gc["gbs"]
     line["roofline"]["frac_of_random_gather_ceiling"] = achieved / gc["gbs"]
     W.release_smoothing()
-    if args.cpu_seconds > 0:
+    if args.cpu_seconds > 0 and world == 1:   # the CPU leg and its parity: rank 0 at N = 1
         line["cpu_baseline"], line["parity"] = cpu_baseline(ht, W, args)
     return line
 
