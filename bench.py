@@ -522,11 +522,13 @@ def run_ours(args, rank, world, device):
                      "peak": peak_bw, "unit": "GB/s", "frac": achieved / peak_bw,
                      "peak_source": peak_kind, "traffic": traffic,
                      "alg_bytes_per_launch": alg_bytes, "cells_walked": cells},
-        # ours per step: per filter the window table + 3 transform kernels (pencil passes,
-        # or the transposed path's window/transpose kernels) and 4 peak-scan kernels; per
-        # step the pencil transpose, pack, order keys, walk, halo flags and records (+
-        # features and MLP in learned mode); cuFFT and CUB launches not counted
-        "gpu_launches": int(args.steps * (8 * nf + (1 if W.pencil else 0) + 5 +
+        # ours per step: per filter the window table (+ its kz rows on the pencil path),
+        # 3 transform kernels (pencil passes, or the transposed path's window/transpose
+        # kernels) and 4 peak-scan kernels; per step the pencil transpose, pack, order keys,
+        # walk, halo flags and records (+ features and MLP in learned mode); cuFFT and CUB
+        # launches not counted
+        "gpu_launches": int(args.steps * ((9 if W.pencil else 8) * nf +
+                                          (1 if W.pencil else 0) + 5 +
                                           (2 if args.mode == "learned" else 0))),
         "clocks": ck,
         "e2e": e2e,

@@ -221,7 +221,7 @@ static void free_ctx(ht_ctx* c) {
     void* ptrs[] = {c->d_off, c->d_start, c->d_count, c->d_r2, c->d_rad, c->d_ct, c->d_akk,
                     c->d_wrow, c->d_wpk, c->d_irad, c->d_irad3, c->d_cell,
                     c->d_rec, c->d_pf_ws, c->d_scratch, c->d_win, c->d_cwork, c->d_order_ws,
-                    c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_ftw, c->d_queue,
+                    c->d_mlp_ws, c->d_cwork2, c->d_tw, c->d_ftw, c->d_wb, c->d_wu, c->d_queue,
                     c->d_stats, c->d_chi, c->d_zchi, c->d_atab, c->d_Da, c->d_dlnD,
                     c->d_cat_ws, c->d_merge_ws, c->d_merge_cells, c->d_merge_scan};
     for (void* p : ptrs)

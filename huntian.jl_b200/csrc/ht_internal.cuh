@@ -88,6 +88,14 @@ struct ht_ctx {
     void* d_ftw = nullptr;         // fused-path twiddles for side fz_n
     size_t ftw_bytes = 0;
     int fz_n = 0;
+    // pencil Z pass window rows: the distinct kx^2 + ky^2 of side wb_n (wb_count of them)
+    // followed by the row index of every (kx, ky); d_wu holds one row of the window along
+    // kz per distinct value, rebuilt for every filter
+    void* d_wb = nullptr;
+    size_t wb_bytes = 0;
+    int wb_n = 0, wb_count = 0;
+    void* d_wu = nullptr;
+    size_t wu_bytes = 0;
     void* d_order_ws = nullptr;    // BATCHED peak-order keys, indices and sort temp
     size_t order_ws_bytes = 0;
     void* d_mlp_ws = nullptr;      // bracket training activations

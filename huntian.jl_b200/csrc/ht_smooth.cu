@@ -42,6 +42,35 @@ __global__ void window_table_kernel(float* __restrict__ tab, int nvals, double d
     tab[q] = (float)(w * scale);
 }
 
+// The window along kz of every distinct b = kx^2 + ky^2 (vals[i], ascending), for the
+// pencil Z pass: U[i * UP + kz] = tab[b + kz^2] for kz <= h = n/2, 0 for h < kz < UP.  A
+// Z-pass column then reads its window as one contiguous row (a 128-byte line per 32
+// values) instead of one line per value (consecutive kz^2 lie more than a line apart
+// beyond kz = 16).  A block takes 32 consecutive distinct values: its lanes read tab at
+// b_lane + kz^2, a few lines per warp since neighbouring distinct b differ by about 5,
+// and the 32 x 32 tile is written back along the rows through shared memory.
+__global__ void __launch_bounds__(256) window_rows_kernel(const float* __restrict__ tab,
+                                                          const int32_t* __restrict__ vals,
+                                                          int nb, int h, int UP,
+                                                          float* __restrict__ U) {
+    __shared__ float s[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;   // block (32, 8)
+    const int i0 = blockIdx.x * 32;
+    const int b = i0 + tx < nb ? __ldg(vals + i0 + tx) : 0;
+    for (int kc = 0; kc < UP; kc += 32) {
+        for (int j = ty; j < 32; j += 8) {
+            const int kz = kc + j;
+            s[j][tx] = (i0 + tx < nb && kz <= h) ? __ldg(tab + (b + kz * kz)) : 0.f;
+        }
+        __syncthreads();
+        for (int r = ty; r < 32; r += 8) {
+            const int kz = kc + tx;
+            if (i0 + r < nb && kz < UP) U[(long long)(i0 + r) * UP + kz] = s[tx][r];
+        }
+        __syncthreads();
+    }
+}
+
 // One thread per mode; grid (ceil((n/2+1) / 256), n, n) so that the mode's (iy, iz)
 // come from the block index instead of 64-bit division.
 __global__ void __launch_bounds__(256) window_apply_kernel(const float2* __restrict__ in,
@@ -658,8 +687,9 @@ __device__ __forceinline__ void pencil_finish(float2* __restrict__ ob,
 template <int T, class Sh>
 __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     const float2* __restrict__ P, float2* __restrict__ B, int NK, int zlo, int Rz,
-    const float* __restrict__ tab, const float2* __restrict__ twL,
-    const float2* __restrict__ tw32, int32_t* __restrict__ status, long long wait_ns) {
+    const float* __restrict__ U, const int32_t* __restrict__ urow, int UP,
+    const float2* __restrict__ twL, const float2* __restrict__ tw32,
+    int32_t* __restrict__ status, long long wait_ns) {
     constexpr int COLS = Sh::cols, N = 32 * T, S = pencil_stride<T, COLS>(), NB = N / COLS,
                   H = T / 2;
     extern __shared__ __align__(128) float2 sm[];
@@ -688,20 +718,17 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) pz_kernel(
     bool ok = true;
     for (; task < ntasks; task += gridDim.x) {
         const int kx = task / NB, ky0 = (task - kx * NB) * COLS, ky = ky0 + w;
-        // Window W(base + sz^2), gathered before the wait (scattered L2 reads that do not
-        // depend on the copy).  Each value is fetched once: kz = lane + 32 t < N/2 for
-        // t < H; the upper half kz' = N - kz (same sz^2) is lane 32 - lane's value at
-        // t' = T - 1 - t, handed over by a shuffle.  Lane 0's upper half kz = 32 t has
-        // |sz| = 32 (T - t): its own lower-half value, or N/2 (wmid) at t = H.
-        const int sy = ky <= N / 2 ? ky : ky - N;
-        const int base = kx * kx + sy * sy;
+        // Window W(kx^2 + sy^2 + sz^2) from the column's row of U (urow: the row of this
+        // (kx, ky)), loaded before the wait (it does not depend on the copy).  Each value
+        // is fetched once: kz = lane + 32 t < N/2 for t < H; the upper half kz' = N - kz
+        // (same sz^2) is lane 32 - lane's value at t' = T - 1 - t, handed over by a
+        // shuffle.  Lane 0's upper half kz = 32 t has |sz| = 32 (T - t): its own lower-
+        // half value, or N/2 (wmid) at t = H.
+        const float* wrow = U + (long long)__ldg(urow + (long long)kx * N + ky) * UP;
         float wl[H];
 #pragma unroll
-        for (int t = 0; t < H; ++t) {
-            const int kz = lane + 32 * t;
-            wl[t] = __ldg(tab + (base + kz * kz));
-        }
-        const float wmid = __ldg(tab + (base + (N / 2) * (N / 2)));
+        for (int t = 0; t < H; ++t) wl[t] = __ldg(wrow + lane + 32 * t);
+        const float wmid = __ldg(wrow + N / 2);
         ok = tid == 0 ? htasync::bar_wait(&bar, parity, wait_ns) : true;
         if (__syncthreads_or(!ok)) {
             ok = false;
@@ -914,6 +941,59 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
 // Tile sides the pencil path handles: n = 32 T with T in {18, 36}.
 static bool pencil_side(int n) { return n == 576 || n == 1152; }
 
+// Row pitch of the window rows U: n/2 + 1 values rounded up to a multiple of 4.
+static int window_row_pitch(int n) { return (n / 2 + 1 + 3) & ~3; }
+
+// Once per side n: the distinct b = kx^2 + sy^2 over the rfft modes (kx <= n/2, sy the
+// signed ky), ascending, then for every (kx, ky) the index of its b among them, in one
+// buffer: [distinct values][row index, kx-major].  103,797 values at n = 1152.
+static int window_rows_index(ht_ctx* ctx, int n, cudaStream_t st) {
+    if (ctx->wb_n == n) return HT_OK;
+    const int h = n / 2, nk = h + 1;
+    const int bmax = 2 * h * h;
+    std::vector<int32_t> at((size_t)bmax + 1, -1);
+    for (int kx = 0; kx < nk; ++kx)
+        for (int sy = 0; sy <= h; ++sy) at[(size_t)kx * kx + (size_t)sy * sy] = 0;
+    std::vector<int32_t> buf;
+    for (int b = 0; b <= bmax; ++b)
+        if (at[b] == 0) {
+            at[b] = (int32_t)buf.size();
+            buf.push_back(b);
+        }
+    const int count = (int)buf.size();
+    buf.resize((size_t)count + (size_t)nk * n);
+    for (int kx = 0; kx < nk; ++kx)
+        for (int ky = 0; ky < n; ++ky) {
+            const int sy = ky <= h ? ky : ky - n;
+            buf[(size_t)count + (size_t)kx * n + ky] = at[(size_t)kx * kx + (size_t)sy * sy];
+        }
+    // the buffer may still be read by a Z pass of the previous side queued on st
+    HT_CUDA_TRY(cudaStreamSynchronize(st), "window row index: stream sync");
+    int rc = ht_grow(&ctx->d_wb, &ctx->wb_bytes, buf.size() * sizeof(int32_t),
+                     "window row index");
+    if (rc != HT_OK) return rc;
+    HT_CUDA_TRY(cudaMemcpy(ctx->d_wb, buf.data(), buf.size() * sizeof(int32_t),
+                           cudaMemcpyHostToDevice), "window row index upload");
+    ctx->wb_n = n;
+    ctx->wb_count = count;
+    return HT_OK;
+}
+
+// Per filter, after the window table: the rows U of every distinct b.
+static int window_rows(ht_ctx* ctx, int n, cudaStream_t st) {
+    int rc = window_rows_index(ctx, n, st);
+    if (rc != HT_OK) return rc;
+    const int UP = window_row_pitch(n);
+    rc = ht_grow(&ctx->d_wu, &ctx->wu_bytes, (size_t)ctx->wb_count * UP * sizeof(float),
+                 "window rows");
+    if (rc != HT_OK) return rc;
+    window_rows_kernel<<<(unsigned)((ctx->wb_count + 31) / 32), dim3(32, 8), 0, st>>>(
+        (const float*)ctx->d_win, (const int32_t*)ctx->d_wb, ctx->wb_count, n / 2, UP,
+        (float*)ctx->d_wu);
+    HT_CUDA_TRY(cudaGetLastError(), "window_rows_kernel launch");
+    return HT_OK;
+}
+
 // Z, Y and X passes from pencils P, through B and C (C may reuse P's buffer: P is read
 // only by the first pass).  Persistent grids: as many CTAs as fit on the device, capped by
 // the work items.
@@ -941,8 +1021,10 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
     const unsigned gz = (unsigned)std::min(zt, sms * bz);
     const unsigned gy = (unsigned)std::min(yt, sms * by);
     const unsigned gx = (unsigned)std::min((rows + 7) / 8, sms * bx);
+    const int32_t* urow = (const int32_t*)ctx->d_wb + ctx->wb_count;
     pz_kernel<T, PencilZ><<<gz, PencilZ::threads, smz, st>>>(
-        P, B, nk, zlo, Rz, (const float*)ctx->d_win, tw.lmL, tw.w32, status, ctx->wait_ns);
+        P, B, nk, zlo, Rz, (const float*)ctx->d_wu, urow, window_row_pitch(n), tw.lmL, tw.w32,
+        status, ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "pz_kernel launch");
     py_kernel<T, PencilY><<<gy, PencilY::threads, smy, st>>>(B, C, nk, nkp, Rz, ylo, Ry,
                                                              tw.lmL, tw.w32, status,
@@ -996,6 +1078,7 @@ static int smooth_pencil_run(ht_ctx* ctx, const float2* P, float* d_out, int n, 
         rc = ht_grow(&ctx->d_cwork, &ctx->cwork_bytes, cbytes, "smoothing buffer");
     if (rc == HT_OK) rc = fused_tables(ctx, n);
     if (rc == HT_OK) rc = scaled_window_table(ctx, n, boxsize, Rf, wsmooth, st);
+    if (rc == HT_OK) rc = window_rows(ctx, n, st);
     if (rc != HT_OK) return rc;
     float2* B = (float2*)ctx->d_cwork2;
     float2* C = (float2*)ctx->d_cwork;
@@ -1003,7 +1086,7 @@ static int smooth_pencil_run(ht_ctx* ctx, const float2* P, float* d_out, int n, 
     rc = n == 1152 ? launch_pencil<36>(ctx, P, B, C, out, zlo, zhi, ylo, yhi, st)
                    : launch_pencil<18>(ctx, P, B, C, out, zlo, zhi, ylo, yhi, st);
     if (rc != HT_OK) return rc;
-    ctx->last_kernels = 4;
+    ctx->last_kernels = 5;
     return HT_OK;
 }
 
@@ -1024,7 +1107,7 @@ static int smooth_tile_pencil(ht_ctx* ctx, const void* d_delta_k, float* d_out, 
     rc = launch_pencil_transpose((const float2*)d_delta_k, P, n, st);
     if (rc != HT_OK) return rc;
     rc = smooth_pencil_run(ctx, P, d_out, n, boxsize, Rf, wsmooth, zlo, zhi, 0, n, st);
-    if (rc == HT_OK) ctx->last_kernels = 5;
+    if (rc == HT_OK) ctx->last_kernels = 6;
     return rc;
 }
 
