@@ -48,24 +48,36 @@ __global__ void window_table_kernel(float* __restrict__ tab, int nvals, double d
 // values) instead of one line per value (consecutive kz^2 lie more than a line apart
 // beyond kz = 16).  A block takes 32 consecutive distinct values: its lanes read tab at
 // b_lane + kz^2, a few lines per warp since neighbouring distinct b differ by about 5,
-// and the 32 x 32 tile is written back along the rows through shared memory.
+// 16 loads per thread in flight (128 kz per round), and the 128 x 32 tile is written back
+// along the rows through shared memory.
 __global__ void __launch_bounds__(256) window_rows_kernel(const float* __restrict__ tab,
                                                           const int32_t* __restrict__ vals,
                                                           int nb, int h, int UP,
                                                           float* __restrict__ U) {
-    __shared__ float s[32][33];
+    constexpr int KC = 128;
+    __shared__ float s[KC][33];
     const int tx = threadIdx.x, ty = threadIdx.y;   // block (32, 8)
     const int i0 = blockIdx.x * 32;
-    const int b = i0 + tx < nb ? __ldg(vals + i0 + tx) : 0;
-    for (int kc = 0; kc < UP; kc += 32) {
-        for (int j = ty; j < 32; j += 8) {
-            const int kz = kc + j;
-            s[j][tx] = (i0 + tx < nb && kz <= h) ? __ldg(tab + (b + kz * kz)) : 0.f;
+    const bool have = i0 + tx < nb;
+    const int b = have ? __ldg(vals + i0 + tx) : 0;
+    for (int kc = 0; kc < UP; kc += KC) {
+#pragma unroll
+        for (int m = 0; m < KC / 8; ++m) {
+            const int j = ty + 8 * m, kz = kc + j;
+            s[j][tx] = (have && kz <= h) ? __ldg(tab + (b + kz * kz)) : 0.f;
         }
         __syncthreads();
-        for (int r = ty; r < 32; r += 8) {
-            const int kz = kc + tx;
-            if (i0 + r < nb && kz < UP) U[(long long)(i0 + r) * UP + kz] = s[tx][r];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const int r = ty + 8 * m;
+            if (i0 + r < nb) {
+                float* row = U + (long long)(i0 + r) * UP + kc;
+#pragma unroll
+                for (int q = 0; q < KC / 32; ++q) {
+                    const int kz = tx + 32 * q;
+                    if (kc + kz < UP) row[kz] = s[kz][r];
+                }
+            }
         }
         __syncthreads();
     }
@@ -678,9 +690,28 @@ __device__ __forceinline__ void pencil_finish(float2* __restrict__ ob,
         htfft::dft32_row(ob + c * S + k2 * 33);
     }
     __syncthreads();
-    for (int e = tid; e < COLS * R; e += 32 * COLS) {
-        const int r = e / COLS, c = e % COLS;
-        if (c < ncol) dst[(long long)r * pitch + c] = ob[c * S + htfft::km_slot<T>(lo + r)];
+    // thread tid stores column c = tid % COLS of rows r = tid / COLS, r + 32, ...; the slot
+    // km_slot(i) = (i mod T) * 33 + i / T of output i = lo + r is advanced by 32 outputs per
+    // step without a division
+    const int c = tid % COLS;
+    if (c < ncol) {
+        constexpr int Q = 32 / T, M = 32 % T;
+        int r = tid / COLS;
+        const int i = lo + r;
+        int k1 = i / T, rem = i - k1 * T;
+        float2* d = dst + (long long)r * pitch + c;
+        const float2* o = ob + c * S;
+        const long long step = 32LL * pitch;
+        for (; r < R; r += 32) {
+            *d = o[rem * 33 + k1];
+            d += step;
+            k1 += Q;
+            rem += M;
+            if (rem >= T) {
+                rem -= T;
+                ++k1;
+            }
+        }
     }
 }
 
