@@ -884,19 +884,22 @@ __global__ void __launch_bounds__(Sh::threads, Sh::ctas) py_kernel(
 // TH = n / 64: the packed rows have M = n / 2 = 32 TH points.  Every warp streams rows
 // r = global warp, + total warps, ... through two slots: row r + stride is copied into the
 // other slot while row r is packed, transformed and stored.  C rows start NKP values apart;
-// a copy takes the first n/2 + 1 values rounded up to even (16 bytes).  The 32-point DFTs
-// of the TH rows of the four-step transform are finished after a transpose through the
-// row's slot, one row per lane (lanes TH..31 idle), instead of across the lanes: a
-// 32-point DFT in registers costs a third of the instructions of five shuffle stages.
+// a copy takes the first n/2 + 1 values rounded up to even (16 bytes).  At TH = 18 the
+// 32-point DFTs of the TH rows of the four-step transform are finished after a transpose
+// through the row's slot, one row per lane (lanes TH..31 idle): a 32-point DFT in
+// registers costs about half the instructions of five shuffle stages over 18 rows.  At
+// TH = 9 the shuffle stages stay (measured faster: 9 busy lanes save little there).
 template <int TH>
 __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
                                                  float2* __restrict__ out, int NKP, int zlo,
                                                  int ylo, int Ry, long long rows,
                                                  const float2* __restrict__ twp,
                                                  const float2* __restrict__ twM,
+                                                 const float2* __restrict__ tw32,
                                                  int32_t* __restrict__ status,
                                                  long long wait_ns) {
     constexpr int M = 32 * TH, N = 2 * M, S = pencil_slot_x<TH>();
+    constexpr bool kRowDft = TH >= 16;
     static_assert(S >= pencil_row_pitch(N) && S >= 33 * TH, "a padded C row must fit a slot");
     extern __shared__ __align__(128) float2 sm[];
     __shared__ __align__(8) unsigned long long bars[8][2];
@@ -916,6 +919,8 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
         }
     }
     __syncwarp();
+    htfft::C2 w32[5];
+    if (!kRowDft) htfft::lane_twiddles(lane, tw32, w32);
     bool ok = true;
     int i = 0;
     for (; r < rows; ++i, r += stride) {
@@ -948,17 +953,26 @@ __global__ void __launch_bounds__(256) px_kernel(const float2* __restrict__ C,
             const float2 o = make_float2(d.x * wv.x - d.y * wv.y, d.x * wv.y + d.y * wv.x);
             v[t] = htfft::to_c2(make_float2(e.x - o.y, e.y + o.x));
         }
-        htfft::warp_ifft_inner<TH>(v, twM, lane);
-        __syncwarp();                          // every lane has read its points of the row
-#pragma unroll
-        for (int k2 = 0; k2 < TH; ++k2) col[k2 * 33 + lane] = make_float2(v[k2].x, v[k2].y);
-        __syncwarp();
-        if (lane < TH) htfft::dft32_row(col + lane * 33);
-        __syncwarp();
         const int zr = (int)(r / Ry), yr = (int)(r - (long long)zr * Ry);
         float2* dst = out + ((long long)(zlo + zr) * N + (ylo + yr)) * M;
-        // output i = lane + 32 t sits at km_slot(i) = (i mod TH) * 33 + i / TH
-        {
+        if constexpr (!kRowDft) {
+            htfft::warp_ifft_regs<TH>(v, twM, lane, w32);
+            __syncwarp();
+            htfft::warp_ifft_store<TH>(col, v, lane);
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < TH; ++t)
+                dst[lane + 32 * t] = col[htfft::lm_slot<TH>(lane + 32 * t)];
+        } else {
+            htfft::warp_ifft_inner<TH>(v, twM, lane);
+            __syncwarp();                      // every lane has read its points of the row
+#pragma unroll
+            for (int k2 = 0; k2 < TH; ++k2)
+                col[k2 * 33 + lane] = make_float2(v[k2].x, v[k2].y);
+            __syncwarp();
+            if (lane < TH) htfft::dft32_row(col + lane * 33);
+            __syncwarp();
+            // output i = lane + 32 t sits at km_slot(i) = (i mod TH) * 33 + i / TH
             constexpr int Q = 32 / TH, MR = 32 % TH;
             int k1 = lane / TH, rem = lane - k1 * TH;
 #pragma unroll
@@ -1078,7 +1092,7 @@ static int launch_pencil(ht_ctx* ctx, const float2* P, float2* B, float2* C, flo
                                                              ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "py_kernel launch");
     px_kernel<TH><<<gx, 256, smx, st>>>(C, d_out, nkp, zlo, ylo, Ry, rows, tw.nat, tw.lmM,
-                                        status, ctx->wait_ns);
+                                        tw.w32, status, ctx->wait_ns);
     HT_CUDA_TRY(cudaGetLastError(), "px_kernel launch");
     return HT_OK;
 }
