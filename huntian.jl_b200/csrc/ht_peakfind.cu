@@ -354,14 +354,23 @@ __global__ void __launch_bounds__(kEmitThreads) pf_emit_kernel(
     __shared__ int warp_tot[kEmitThreads / 32];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const long long w0 = (long long)blockIdx.x * kSegWords + (long long)tid * kWordsPerThread;
+    const long long seg0 = __ldg(segbase + blockIdx.x);   // in flight with the words
     uint32_t words[kWordsPerThread];
+    static_assert(kWordsPerThread == 8, "two 16-byte loads per thread");
+    if (w0 + kWordsPerThread <= g.nwords) {
+        // 32-byte aligned: the workspace is, and w0 is a multiple of 8 words
+        const uint4 a = __ldg(reinterpret_cast<const uint4*>(bits + w0));
+        const uint4 b = __ldg(reinterpret_cast<const uint4*>(bits + w0 + 4));
+        words[0] = a.x; words[1] = a.y; words[2] = a.z; words[3] = a.w;
+        words[4] = b.x; words[5] = b.y; words[6] = b.z; words[7] = b.w;
+    } else {
+#pragma unroll
+        for (int t = 0; t < kWordsPerThread; ++t)
+            words[t] = w0 + t < g.nwords ? bits[w0 + t] : 0u;
+    }
     int c = 0;
 #pragma unroll
-    for (int t = 0; t < kWordsPerThread; ++t) {
-        const long long w = w0 + t;
-        words[t] = w < g.nwords ? bits[w] : 0u;
-        c += __popc(words[t]);
-    }
+    for (int t = 0; t < kWordsPerThread; ++t) c += __popc(words[t]);
     // block exclusive scan of c
     int x = c;
 #pragma unroll
@@ -373,7 +382,7 @@ __global__ void __launch_bounds__(kEmitThreads) pf_emit_kernel(
     __syncthreads();
     int wbase = 0;
     for (int i = 0; i < wid; ++i) wbase += warp_tot[i];
-    long long slot = segbase[blockIdx.x] + wbase + x - c;
+    long long slot = seg0 + wbase + x - c;
     if (c == 0 || slot >= max_peaks) return;
     const long long n = g.n, nn = n * n;
 #pragma unroll
