@@ -120,7 +120,7 @@ def test_precompute_shells(oracle):
         rows = c2[c2[:, 3] == r2][:, :3]
         keys = [tuple(x) for x in rows[:, ::-1]]
         assert keys == sorted(keys)
-    # shell counts of the hunt radii the configurations use (probed in the survey)
+    # shell counts of the hunt radii the configurations use (8, 24 and 35 cells)
     for rmax, ncells, nsh in [(8, 2109, 55), (24, 57777, 482), (35, 179579, 1024)]:
         c = oracle.precompute_shells(rmax)
         st, cnt, r2 = oracle.build_shell_tables(c)
